@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Throughput of the KMA device heap on the fragmentation stress workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step): config 2 -- a 1 GiB heap of 16 KiB superblocks, 148 x
+2048 work-items, 64 rounds; each round every item mallocs 8 << U{0..8}
+bytes, tags every word of the block with its id, then frees a seeded 50%
+of its live blocks after verifying their tags; after the last round the
+live set is drained.  A step is reset + seed + rounds + drain on a heap
+resident in HBM.  op = one malloc call or one free call.
+
+Our arm times K steps with CUDA events on the launching stream (L2 flushed
+between steps, outside the timed events), max over ranks; N > 1 runs
+independent per-GPU heap replicas (weak scaling: the heap does not shard
+and has no exchange step).  It also reports the plain per-thread kernel on
+the same GPU, the roofline of the dominant kernel, the CPU baseline, the
+end-to-end figure through the host-buffer C ABI call, and the invariant
+check of one extra step.  The reference arm times the reference's own
+kma.cl built as host C (oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "M malloc+free ops/s on 1 B200 (0 heap-invariant faults); p99 serving latency"
+UNIT = "Mops/s"
+ITEMS = 148 * 2048
+ROUNDS = 64
+SBLOCKS = 65536
+SB_LOG2 = 14
+SEED = 0xC2
+MEAN_REQ = (8 + 16 + 32 + 64 + 128 + 256 + 512 + 1024 + 2048) / 9.0
+WORKLOAD = ("C2 fragmentation stress: 1 GiB heap of 16 KiB superblocks, 148x2048 items, 64 rounds, "
+            "malloc 8<<U{0..8} B per round, seeded 50% frees of the live set, every word tagged and "
+            "verified; step = reset + seed + rounds + drain")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "c2_rounds_warp_traffic.json")
+
+
+def peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return {"hbm_gbs": float(p["hbm_gbs"]), "src": "measured"}
+    except Exception:  # noqa: BLE001 - file absent: the recipe's fallback
+        return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu)],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+# ---------------------------------------------------------------- CPU legs
+def cpu_run(kind_pref: str, items: int, threads: int, timeout: float) -> dict:
+    """Run the reference's kma.cl (oracle/_ref; the C restatement when the
+    reference build is absent) on `threads` host threads over `items`
+    work-items of the workload, in a child process with a time limit."""
+    code = f"""
+import json, sys
+sys.path.insert(0, {ROOT!r})
+from oracle import oracle
+kind = "reference" if oracle.ref_available({SB_LOG2}) and {kind_pref!r} == "reference" else "port"
+H = oracle.Ref if kind == "reference" else oracle.Port
+with H({SBLOCKS}, {SB_LOG2}) as h:
+    st = h.run_workload(2, {items}, {ROUNDS}, {SEED}, 2, {threads})
+st["kind"] = kind
+print(json.dumps(st))
+"""
+    try:
+        r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                           timeout=timeout)
+        if r.returncode != 0:
+            return {"error": r.stderr.strip().splitlines()[-1:]}
+        return json.loads(r.stdout.strip().splitlines()[-1])
+    except subprocess.TimeoutExpired:
+        return {"error": f"timed out after {timeout:.0f} s"}
+
+
+def run_reference(args) -> int:
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    items = ITEMS // 4
+    vals = []
+    last = None
+    for k in range(args.warmup + args.steps):
+        st = cpu_run("reference", items, threads, timeout=120)
+        if "error" in st:
+            print(json.dumps({"impl": "reference", "unavailable": f"CPU run failed: {st['error']}"}))
+            return 0
+        if k >= args.warmup:
+            vals.append((st["mallocs"] + st["frees"]) / st["seconds"] / 1e6)
+            last = st
+    v = statistics.median(vals)
+    kind = last["kind"]
+    sample = (f"{items} of the {ITEMS} work-items x {ROUNDS} rounds per step (1 GiB heap, 16 KiB "
+              f"superblocks), work-items round-robin on {threads} pthreads, each to completion; "
+              f"{'kma.cl+clIndexedQueue.cl built unmodified as host C' if kind == 'reference' else 'C restatement of kma.cl'}")
+    line = {"metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * last["seconds"], 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "items_per_step": items, "rounds": ROUNDS,
+                       "heap_bytes": SBLOCKS << SB_LOG2, "sb_size": 1 << SB_LOG2,
+                       "invariant_faults": int(last["bad_tags"]), "nulls": int(last["nulls"])},
+            "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_ours(args) -> int:
+    import numpy as np
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from kma_b200 import MODE_PLAIN, MODE_WARP, WL_C2, Heap, Workload, bench_atomics
+    from kma_b200 import inspect as ins
+
+    mode = MODE_WARP if args.mode == "warp" else MODE_PLAIN
+    stream = torch.cuda.current_stream()
+    heap = Heap(SBLOCKS, SB_LOG2, stream=stream)
+    wl = Workload(heap, WL_C2, ITEMS)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step(m, ev=None):
+        if ev:
+            ev[0].record(stream)
+        heap.reset(stream)
+        wl.begin(SEED, stream)
+        if ev:
+            ev[1].record(stream)
+        wl.rounds(ROUNDS, m, stream=stream)
+        if ev:
+            ev[2].record(stream)
+        wl.drain(m, stream=stream)
+        if ev:
+            ev[3].record(stream)
+
+    def timed(m, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            step(m)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
+        if sampler:
+            sampler.start()
+        for k in range(steps):
+            flush.zero_()  # > L2, outside the timed events
+            step(m, evs[k])
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        if world > 1:
+            torch.distributed.barrier()
+        step_ms = [e[0].elapsed_time(e[3]) for e in evs]
+        rounds_ms = [e[1].elapsed_time(e[2]) for e in evs]
+        return step_ms, rounds_ms, clocks
+
+    sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
+                           if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit()
+                           else local)
+    step_ms, rounds_ms, clocks = timed(mode, args.steps, args.warmup, sampler)
+    st = wl.stats(stream)
+    ops_step = st["mallocs"] + st["frees"]
+    total_ms = sum(step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = world * ops_step * args.steps / (total_ms / 1e3) / 1e6
+
+    out = None
+    if rank == 0:
+        # bytes of the rounds launch (deterministic when no malloc returns NULL)
+        heap.reset(stream)
+        wl.begin(SEED, stream)
+        wl.rounds(ROUNDS, mode, stream=stream)
+        st_r = wl.stats(stream)
+        # one checked step: live-block invariants, then drain to canonical empty
+        nlive, off, size = wl.live(stream)
+        sel = np.arange(off.shape[0])[:, None] < nlive[None, :]
+        res = ins.check_live_blocks(heap.snapshot(stream=stream), off[sel], size[sel],
+                                    heap.bitmaps(stream))
+        wl.drain(mode, stream=stream)
+        st_d = wl.stats(stream)
+        empty = ins.check_canonical_empty(heap.snapshot(stream=stream), heap.bitmaps(stream))
+        faults = ins.violations(res) + len(empty) + int(st_d["bad_tags"]) + int(st["bad_tags"])
+        flags = heap.error_flags(clear=True, stream=stream)
+
+        rounds_bytes = st_r["fill_bytes"] + st_r["verify_bytes"]
+        rounds_ops = st_r["mallocs"] + st_r["frees"]
+        mean_rounds_s = statistics.mean(rounds_ms) / 1e3
+        pk = peaks()
+        achieved = rounds_bytes / mean_rounds_s / 1e9
+        traffic = None
+        if os.path.exists(PROFILE_TRAFFIC):
+            try:
+                traffic = json.load(open(PROFILE_TRAFFIC)).get("traffic_bytes_per_launch")
+            except Exception:  # noqa: BLE001
+                traffic = None
+        # measured L2 atomic peak (distinct 128-byte lines, returning atomicAdd)
+        n_at = 148 * 2048
+        at_ms = bench_atomics(True, n_at, 64, 32, stream=stream)
+        p_atom = n_at * 64 / (at_ms / 1e3)
+        at_same_ms = bench_atomics(False, 148 * 256, 16, 32, stream=stream)
+        p_same = 148 * 256 * 16 / (at_same_ms / 1e3)
+        op_rate = rounds_ops / mean_rounds_s
+
+        # plain per-thread kernel on the same GPU (the >=5x denominator)
+        plain = None
+        if not args.no_plain and mode != MODE_PLAIN:
+            p_ms, _, _ = timed(MODE_PLAIN, 2, 1)
+            st_p = wl.stats(stream)
+            plain = (st_p["mallocs"] + st_p["frees"]) / (statistics.mean(p_ms) / 1e3) / 1e6
+
+        # end to end through the host-buffer C ABI call (pinned seeds in,
+        # per-item hashes + counters out)
+        g = np.arange(ITEMS, dtype=np.uint64)
+        seeds_np = np.uint64(SEED) ^ (g * np.uint64(0x9E3779B97F4A7C15))
+        seeds = torch.from_numpy(seeds_np.view(np.int64)).pin_memory()
+        hashes = torch.empty(ITEMS, dtype=torch.int64).pin_memory()
+        wl.run_host(seeds.data_ptr(), ROUNDS, mode, hashes.data_ptr(), stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            st_e = wl.run_host(seeds.data_ptr(), ROUNDS, mode, hashes.data_ptr(), stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / args.steps
+        e2e = {"value": round((st_e["mallocs"] + st_e["frees"]) / (e2e_ms / 1e3) / 1e6, 3),
+               "unit": UNIT, "h2d_bytes_per_step": ITEMS * 8,
+               "d2h_bytes_per_step": ITEMS * 8 + 56,
+               "ms_per_step": round(e2e_ms, 3),
+               "call": "kma_wl_run_host (host seeds in, host hashes + counters out)"}
+
+        cpu = None
+        if not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            items = ITEMS // 4
+            c = cpu_run("reference", items, threads, timeout=120)
+            if "error" not in c:
+                cpu = {"value": round((c["mallocs"] + c["frees"]) / c["seconds"] / 1e6, 3),
+                       "unit": UNIT, "cores": threads, "kind": c["kind"],
+                       "sample": f"{items} of {ITEMS} work-items x {ROUNDS} rounds, round-robin on "
+                                 f"{threads} pthreads (the reference's kma.cl as host C); "
+                                 f"its own tag faults: {c['bad_tags']}"}
+            else:
+                cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+                       "sample": f"unavailable: {c['error']}"}
+
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "mode": args.mode, "items": ITEMS, "rounds": ROUNDS,
+                       "heap_bytes": SBLOCKS << SB_LOG2, "sb_size": 1 << SB_LOG2,
+                       "ops_per_step": ops_step, "nulls": int(st["nulls"]),
+                       "invariant_faults": faults, "heap_error_flags": flags,
+                       "l2": "inputs larger than L2 (1 GiB heap) and a 256 MiB write between "
+                             "steps, outside the timed events",
+                       "parallelism": f"replicas x{world}",
+                       "plain_mops": round(plain, 3) if plain else None,
+                       "warp_over_plain": round(value / world / plain, 2) if plain else None},
+            "roofline": {"bound": "hbm", "kernel": "k_wl_rounds<warp>",
+                         "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": round(achieved / pk["hbm_gbs"], 4), "traffic": traffic,
+                         "peak_src": pk["src"],
+                         "algorithmic_bytes_per_launch": rounds_bytes,
+                         "launch_ms": round(1e3 * mean_rounds_s, 3)},
+            "l2_atomic": {"achieved": round(op_rate / 1e9, 3), "peak": round(p_atom / 1e9, 3),
+                          "unit": "G atomics/s", "frac": round(op_rate / p_atom, 4),
+                          "same_address_peak": round(p_same / 1e9, 3),
+                          "note": "algorithmic 2 L2 atomics per malloc+free pair = 1 per op; "
+                                  "peak = returning atomicAdd on distinct 128-B lines, all SMs"},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 4 * args.steps, "clocks": clocks,
+        }
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    wl.close()
+    heap.close()
+    if out is not None:
+        print(json.dumps(out))
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["warp", "plain"], default="warp")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-kernel comparison")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,768 @@
+/*
+ * kma_device.cuh -- device-side API of the B200 KMA heap (sm_100a).
+ *
+ * Drop-in for the reference's device API (clheap.h:37-39, kma.cl:279-373):
+ *   void *kma_malloc(kma_heap *heap, size_t size);   NULL on failure
+ *   void  kma_free(kma_heap *heap, void *p);         kma_free(h, NULL) is a no-op
+ * plus warp-collaborative forms (any subset of a warp may call them, with
+ * different sizes per lane):
+ *   void *kma_malloc_warp(kma_heap *heap, size_t size);
+ *   void  kma_free_warp(kma_heap *heap, void *p);
+ * and the lock-free structures (kma_structs.cuh): clqueue, clindexedqueue,
+ * cltree, clarraylist, and the PMA bump heap (pma_malloc/pma_free).
+ *
+ * Heap layout in HBM (one cudaMalloc per heap, owned by kma_create):
+ *   [kma_heap header | sb_state[nsb] u32 | sb_next[nsb] u64 | superblocks]
+ *   superblock s at sb_base + s*SB: bytes [0,12) reserved (keeps every block
+ *   offset identical to the reference's in-band 12-byte header, kma.h:71-78),
+ *   blocks from +12, allocation bitmap at the tail growing downward
+ *   (bitmap word k = slots 32k..32k+31 at u32 index SB/4-1-k, kma.cl:183-188).
+ *   The superblock header fields live in coalesced side arrays instead:
+ *   sb_state[s] = class<<28 | slots<<14 | free  (the reference packs
+ *   slots<<16 | free, kma.cl:180; the class field is what makes a stale
+ *   reservation detectable), sb_next[s] = tagged free-list link.
+ * Class table cls[c] (kma.h:84): 0 empty, 1 POISON (refill in progress),
+ * s+2 = superblock s is the current one for class c.  Each hot word sits on
+ * its own 128-byte line.
+ *
+ * Every spin (POISON wait, CAS retry, queue helpers) is bounded by
+ * heap->spin_limit iterations; on expiry the call fails (NULL / 0), sets
+ * KMA_ERR_TIMEOUT in heap->err and never traps.
+ */
+#ifndef KMA_DEVICE_CUH
+#define KMA_DEVICE_CUH
+
+#include <stdint.h>
+#include <stddef.h>
+
+#define KMA_MAX_CLASSES 16
+#define KMA_SB_HDR 12u
+#define KMA_POISON 1u
+#define KMA_CLS_BASE 2u
+
+#define KMA_ST_FREE_MASK 0x3fffu
+#define KMA_ST_SLOTS_SHIFT 14
+#define KMA_ST_CLASS_SHIFT 28
+
+/* heap->err bits */
+#define KMA_ERR_TIMEOUT 1u
+#define KMA_ERR_BADFREE 2u
+
+struct __align__(128) kma_line32 {
+	uint32_t v;
+	uint32_t pad_[31];
+};
+struct __align__(128) kma_line64 {
+	unsigned long long v;
+	unsigned long long pad_[15];
+};
+
+struct __align__(128) kma_heap {
+	/* geometry: written by kma_create, read-only afterwards */
+	unsigned char *sb_base;
+	uint32_t *sb_state;
+	unsigned long long *sb_next;
+	unsigned long long region_bytes; /* nsb << sb_log2 */
+	uint32_t sb_log2;
+	uint32_t sb_size;
+	uint32_t nsb;        /* superblocks allocated (the reference's sblocks) */
+	uint32_t pages;      /* superblocks on the free list: sblocks-1 (kma.cl:42) */
+	uint32_t nclasses;   /* KMA_SB_SIZE_BUCKETS = log2 - 1 (kma.h:29) */
+	uint32_t max_request;/* SB - 16 (kma.cl:126) */
+	uint32_t spin_limit;
+	uint32_t flags;
+	uint32_t cls_size[KMA_MAX_CLASSES];  /* kma.cl:55-90 */
+	uint32_t cls_slots[KMA_MAX_CLASSES]; /* kma.cl:95-113 */
+	uint32_t cls_magic[KMA_MAX_CLASSES]; /* floor(2^32/size)+1: exact x/size for x < 2^16 */
+	uint32_t cls_words[KMA_MAX_CLASSES]; /* bitmap words = ceil(slots/32) */
+	/* hot words, one line each */
+	kma_line64 free_head;
+	kma_line64 free_tail;
+	kma_line32 cls[KMA_MAX_CLASSES];
+	kma_line32 err;
+};
+
+/* ------------------------------------------------------------------ */
+/* memory-model helpers (gpu scope)                                    */
+/* ------------------------------------------------------------------ */
+namespace kma_detail {
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p)
+{
+	uint32_t v;
+	asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p)
+{
+	uint32_t v;
+	asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p)
+{
+	unsigned long long v;
+	asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ void st_relaxed(uint32_t *p, uint32_t v)
+{
+	asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_release(uint32_t *p, uint32_t v)
+{
+	asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_release64(unsigned long long *p, unsigned long long v)
+{
+	asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t cas_acqrel(uint32_t *p, uint32_t cmp, uint32_t val)
+{
+	uint32_t old;
+	asm volatile("atom.acq_rel.gpu.global.cas.b32 %0, [%1], %2, %3;"
+		     : "=r"(old) : "l"(p), "r"(cmp), "r"(val) : "memory");
+	return old;
+}
+__device__ __forceinline__ unsigned long long cas64_acqrel(unsigned long long *p,
+		unsigned long long cmp, unsigned long long val)
+{
+	unsigned long long old;
+	asm volatile("atom.acq_rel.gpu.global.cas.b64 %0, [%1], %2, %3;"
+		     : "=l"(old) : "l"(p), "l"(cmp), "l"(val) : "memory");
+	return old;
+}
+__device__ __forceinline__ uint32_t add_acqrel(uint32_t *p, uint32_t v)
+{
+	uint32_t old;
+	asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+		     : "=r"(old) : "l"(p), "r"(v) : "memory");
+	return old;
+}
+__device__ __forceinline__ uint32_t or_acqrel(uint32_t *p, uint32_t v)
+{
+	uint32_t old;
+	asm volatile("atom.acq_rel.gpu.global.or.b32 %0, [%1], %2;"
+		     : "=r"(old) : "l"(p), "r"(v) : "memory");
+	return old;
+}
+__device__ __forceinline__ uint32_t and_acqrel(uint32_t *p, uint32_t v)
+{
+	uint32_t old;
+	asm volatile("atom.acq_rel.gpu.global.and.b32 %0, [%1], %2;"
+		     : "=r"(old) : "l"(p), "r"(v) : "memory");
+	return old;
+}
+__device__ __forceinline__ void fence_acqrel()
+{
+	asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t lane_id()
+{
+	uint32_t l;
+	asm volatile("mov.u32 %0, %%laneid;" : "=r"(l));
+	return l;
+}
+__device__ __forceinline__ uint32_t lanemask_lt()
+{
+	uint32_t m;
+	asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+	return m;
+}
+/* position of the n-th (0-based) set bit of m, counting from bit 0;
+ * requires n < popc(m) */
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t n)
+{
+	uint32_t pos = 0;
+#pragma unroll
+	for (uint32_t w = 16; w > 0; w >>= 1) {
+		uint32_t c = __popc((m >> pos) & ((1u << w) - 1u));
+		if (n >= c) {
+			n -= c;
+			pos += w;
+		}
+	}
+	return pos;
+}
+__device__ __forceinline__ void backoff(uint32_t it)
+{
+	if (it > 4)
+		__nanosleep(it < 64 ? 32u : 256u);
+}
+__device__ __forceinline__ void set_err(kma_heap *h, uint32_t e)
+{
+	atomicOr(&h->err.v, e);
+}
+
+/* state word */
+__device__ __forceinline__ uint32_t st_free(uint32_t s) { return s & KMA_ST_FREE_MASK; }
+__device__ __forceinline__ uint32_t st_slots(uint32_t s) { return (s >> KMA_ST_SLOTS_SHIFT) & KMA_ST_FREE_MASK; }
+__device__ __forceinline__ uint32_t st_class(uint32_t s) { return s >> KMA_ST_CLASS_SHIFT; }
+__device__ __forceinline__ uint32_t st_make(uint32_t c, uint32_t slots, uint32_t fr)
+{
+	return (c << KMA_ST_CLASS_SHIFT) | (slots << KMA_ST_SLOTS_SHIFT) | fr;
+}
+
+/* tagged index words {tag:32 | idx:32}, idx 0 = null, idx = item + 1 */
+__device__ __forceinline__ uint32_t tw_idx(unsigned long long w) { return (uint32_t)w; }
+__device__ __forceinline__ uint32_t tw_tag(unsigned long long w) { return (uint32_t)(w >> 32); }
+__device__ __forceinline__ unsigned long long tw_make(uint32_t tag, uint32_t idx)
+{
+	return ((unsigned long long)tag << 32) | idx;
+}
+
+/* bitmap word k of superblock sb (u32 index SB/4-1-k from the SB start) */
+__device__ __forceinline__ uint32_t *bitmap_word(const kma_heap *h, unsigned char *sb, uint32_t k)
+{
+	return reinterpret_cast<uint32_t *>(sb + h->sb_size) - 1 - k;
+}
+
+} /* namespace kma_detail */
+
+/* ------------------------------------------------------------------ */
+/* size classes (kma.cl:55-148)                                        */
+/* ------------------------------------------------------------------ */
+
+/* The reference's _kma_sbid_by_size (kma.cl:119-148) returns the smallest
+ * class whose block size is >= size (its MSB approximation never starts
+ * above that class, and it only ever walks up); sizes above SB-16 give -1.
+ * Sizes 0..3 read an uninitialised variable there; here they map to
+ * class 0, which is what a zero-initialised reference build returns. */
+__device__ __forceinline__ int kma_class_of(const kma_heap *h, size_t size)
+{
+	if (size > __ldg(&h->max_request))
+		return -1;
+	uint32_t s = (uint32_t)size;
+	int c = s < 4 ? 0 : (int)(29 - __clz(s)); /* floor(log2 s) - 2 */
+	while (__ldg(&h->cls_size[c]) < s)
+		c++;
+	return c;
+}
+
+/* ------------------------------------------------------------------ */
+/* superblock free list: MS queue with a dummy node over superblock     */
+/* indices (clIndexedQueue.cl:194-290), links in sb_next[], 64-bit      */
+/* {tag:32|idx:32} words (ABA-safe).  Dequeue returns the OLD dummy, as */
+/* the reference does (clIndexedQueue.cl:282-289), so the first         */
+/* superblock handed out is superblock 0.                               */
+/* ------------------------------------------------------------------ */
+namespace kma_detail {
+
+/* Enqueue superblock s.  Returns 1, or 0 on spin-limit expiry. */
+__device__ __forceinline__ int sb_enqueue(kma_heap *h, uint32_t s)
+{
+	unsigned long long *link = &h->sb_next[s];
+	uint32_t idx = s + 1;
+	unsigned long long old = *((volatile unsigned long long *)link);
+	st_release64(link, tw_make(tw_tag(old) + 1, 0));
+	uint32_t lim = h->spin_limit;
+	for (uint32_t it = 0; it < lim; it++) {
+		unsigned long long t = ld_acquire64(&h->free_tail.v);
+		unsigned long long *tl = &h->sb_next[tw_idx(t) - 1];
+		unsigned long long n = ld_acquire64(tl);
+		if (t != ld_acquire64(&h->free_tail.v))
+			continue;
+		if (tw_idx(n) == 0) {
+			if (cas64_acqrel(tl, n, tw_make(tw_tag(n) + 1, idx)) == n) {
+				cas64_acqrel(&h->free_tail.v, t, tw_make(tw_tag(t) + 1, idx));
+				return 1;
+			}
+		} else {
+			cas64_acqrel(&h->free_tail.v, t, tw_make(tw_tag(t) + 1, tw_idx(n)));
+		}
+		backoff(it);
+	}
+	set_err(h, KMA_ERR_TIMEOUT);
+	return 0;
+}
+
+/* Dequeue: returns the superblock index, or -1 when only the dummy is
+ * left (empty), or -2 on spin-limit expiry. */
+__device__ __forceinline__ int64_t sb_dequeue(kma_heap *h)
+{
+	uint32_t lim = h->spin_limit;
+	for (uint32_t it = 0; it < lim; it++) {
+		unsigned long long hd = ld_acquire64(&h->free_head.v);
+		unsigned long long t = ld_acquire64(&h->free_tail.v);
+		unsigned long long n = ld_acquire64(&h->sb_next[tw_idx(hd) - 1]);
+		if (hd != ld_acquire64(&h->free_head.v))
+			continue;
+		if (tw_idx(hd) == tw_idx(t)) {
+			if (tw_idx(n) == 0)
+				return -1;
+			cas64_acqrel(&h->free_tail.v, t, tw_make(tw_tag(t) + 1, tw_idx(n)));
+		} else if (cas64_acqrel(&h->free_head.v, hd, tw_make(tw_tag(hd) + 1, tw_idx(n))) == hd) {
+			return (int64_t)tw_idx(hd) - 1;
+		}
+		backoff(it);
+	}
+	set_err(h, KMA_ERR_TIMEOUT);
+	return -2;
+}
+
+/* Prepare superblock s for class c: zero its bitmap except the bits in
+ * [pre_lo, slots) which are pre-set (claimed by the refiller), then
+ * publish state = (c, slots, free).  kma.cl:177-189, with the bitmap
+ * written before the state becomes visible. */
+__device__ __forceinline__ void sb_format(kma_heap *h, uint32_t s, uint32_t c, uint32_t pre_lo,
+		uint32_t fr)
+{
+	unsigned char *sb = h->sb_base + ((size_t)s << h->sb_log2);
+	uint32_t slots = h->cls_slots[c];
+	uint32_t words = h->cls_words[c];
+	for (uint32_t k = 0; k < words; k++) {
+		uint32_t lo = k * 32, hi = lo + 32;
+		uint32_t v = 0;
+		if (pre_lo < hi && slots > lo) {
+			uint32_t a = pre_lo > lo ? pre_lo : lo;
+			uint32_t b = slots < hi ? slots : hi;
+			if (b > a) {
+				uint32_t n = b - a;
+				v = (n == 32 ? 0xffffffffu : ((1u << n) - 1u)) << (a - lo);
+			}
+		}
+		*bitmap_word(h, sb, k) = v;
+	}
+	fence_acqrel();
+	st_release(&h->sb_state[s], st_make(c, slots, fr));
+}
+
+} /* namespace kma_detail */
+
+/* ------------------------------------------------------------------ */
+/* plain per-thread malloc/free: the reference algorithm                */
+/* (kma.cl:150-373) with its atomics, made safe against recycling:      */
+/*  - a reservation CAS only succeeds on a state word whose class field */
+/*    is the requested class (a stale cursor whose superblock was       */
+/*    recycled for another class fails and retries);                   */
+/*  - taking the last free slot detaches with CAS(cls, cursor, 0), not  */
+/*    an unconditional exchange (kma.cl:217).                           */
+/* In one-thread-at-a-time execution both are identical to the         */
+/* reference, so serial replay returns the reference's offsets.         */
+/* ------------------------------------------------------------------ */
+namespace kma_detail {
+
+/* kma.cl:232-273: claim a bitmap bit at or above `hint` (wrapping),
+ * write the hint into word 0 of the block. */
+__device__ __forceinline__ void *sb_get_block(kma_heap *h, uint32_t s, uint32_t c, uint32_t hint)
+{
+	unsigned char *sb = h->sb_base + ((size_t)s << h->sb_log2);
+	uint32_t slots = h->cls_slots[c];
+	uint32_t size = h->cls_size[c];
+	uint32_t words = h->cls_words[c];
+	uint32_t slot = hint;
+	uint32_t lim = h->spin_limit;
+	for (uint32_t it = 0; it < lim; it++) {
+		uint32_t k = slot >> 5;
+		uint32_t *wp = bitmap_word(h, sb, k);
+		uint32_t v = ld_relaxed(wp);
+		uint32_t valid = (k == words - 1 && (slots & 31)) ? ((1u << (slots & 31)) - 1u) : 0xffffffffu;
+		uint32_t cand = ~v & valid & (0xffffffffu << (slot & 31));
+		while (cand) {
+			uint32_t b = __ffs(cand) - 1;
+			uint32_t bit = 1u << b;
+			uint32_t old = or_acqrel(wp, bit);
+			if (!(old & bit)) {
+				unsigned char *p = sb + KMA_SB_HDR + (size_t)(k * 32 + b) * size;
+				*reinterpret_cast<uint32_t *>(p) = hint;
+				return p;
+			}
+			cand &= ~old;
+			cand &= ~bit;
+		}
+		slot = (k + 1) * 32;
+		if (slot >= slots)
+			slot = 0;
+	}
+	set_err(h, KMA_ERR_TIMEOUT);
+	return NULL;
+}
+
+} /* namespace kma_detail */
+
+/* kma.cl:279-303 (with _kma_reserve_block, kma.cl:150-225) */
+__device__ inline void *kma_malloc(kma_heap *h, size_t size)
+{
+	using namespace kma_detail;
+	int c = kma_class_of(h, size);
+	if (c < 0)
+		return NULL;
+	uint32_t *clsw = &h->cls[c].v;
+	uint32_t lim = h->spin_limit;
+	for (uint32_t it = 0; it < lim; it++) {
+		/* kma.cl:163: CAS 0 -> POISON doubles as the read of the slot */
+		uint32_t cur = cas_acqrel(clsw, 0, KMA_POISON);
+		if (cur == 0) {
+			/* refill, kma.cl:166-195 */
+			int64_t s = sb_dequeue(h);
+			if (s < 0) {
+				atomicExch(clsw, 0);
+				return NULL;
+			}
+			uint32_t slots = h->cls_slots[c];
+			sb_format(h, (uint32_t)s, c, slots, slots - 1);
+			/* kma.cl:191 publishes the superblock even when the refill
+			 * took its only slot (1-slot classes); every later request
+			 * of that class then spins on a full superblock until the
+			 * block is freed (kma.cl:203-204).  Leave the class empty
+			 * instead, which is what taking the last slot does. */
+			cas_acqrel(clsw, KMA_POISON, slots == 1 ? 0u : (uint32_t)s + KMA_CLS_BASE);
+			return sb_get_block(h, (uint32_t)s, c, slots - 1);
+		}
+		if (cur == KMA_POISON) {
+			backoff(it);
+			continue;
+		}
+		uint32_t s = cur - KMA_CLS_BASE;
+		uint32_t *stp = &h->sb_state[s];
+		/* kma.cl:198 reads the state with atom_add(.., 0) */
+		uint32_t st = add_acqrel(stp, 0);
+		if (st_class(st) != (uint32_t)c || st_free(st) == 0)
+			continue;
+		uint32_t fr = st_free(st) - 1;
+		if (cas_acqrel(stp, st, st - 1) != st)
+			continue;
+		if (fr == 0)
+			cas_acqrel(clsw, cur, 0); /* kma.cl:216-218 */
+		return sb_get_block(h, s, c, fr);
+	}
+	set_err(h, KMA_ERR_TIMEOUT);
+	return NULL;
+}
+
+namespace kma_detail {
+/* Locate the superblock / class / slot of a live block. */
+__device__ __forceinline__ bool block_locate(const kma_heap *h, const void *p, uint32_t &s,
+		uint32_t &c, uint32_t &slot)
+{
+	size_t off = (const unsigned char *)p - h->sb_base;
+	if (off >= h->region_bytes)
+		return false;
+	s = (uint32_t)(off >> h->sb_log2);
+	uint32_t in = (uint32_t)(off & (h->sb_size - 1));
+	uint32_t st = ld_relaxed(&h->sb_state[s]);
+	c = st_class(st);
+	if (st == 0 || in < KMA_SB_HDR || c >= h->nclasses)
+		return false;
+	slot = (uint32_t)(((unsigned long long)(in - KMA_SB_HDR) * h->cls_magic[c]) >> 32);
+	return slot < h->cls_slots[c];
+}
+
+/* Return superblock s (class c) to the free list once all its slots are
+ * free: kma.cl:362-367. */
+__device__ __forceinline__ void sb_recycle(kma_heap *h, uint32_t s, uint32_t c)
+{
+	cas_acqrel(&h->cls[c].v, s + KMA_CLS_BASE, 0);
+	sb_enqueue(h, s);
+}
+} /* namespace kma_detail */
+
+/* kma.cl:305-373 */
+__device__ inline void kma_free(kma_heap *h, void *p)
+{
+	using namespace kma_detail;
+	if (p == NULL)
+		return;
+	uint32_t s, c, slot;
+	if (!block_locate(h, p, s, c, slot)) {
+		set_err(h, KMA_ERR_BADFREE);
+		return;
+	}
+	unsigned char *sb = h->sb_base + ((size_t)s << h->sb_log2);
+	uint32_t bit = 1u << (slot & 31);
+	/* kma.cl:336-338: the old bitmap word lands in word 0 of the block */
+	uint32_t old = and_acqrel(bitmap_word(h, sb, slot >> 5), ~bit);
+	*reinterpret_cast<volatile uint32_t *>(p) = old;
+	if (!(old & bit)) {
+		/* double free: the reference increments the free count anyway
+		 * and corrupts the superblock (kma.cl:333-335); refuse it */
+		set_err(h, KMA_ERR_BADFREE);
+		return;
+	}
+	uint32_t *stp = &h->sb_state[s];
+	uint32_t lim = h->spin_limit;
+	for (uint32_t it = 0; it < lim; it++) {
+		uint32_t st = add_acqrel(stp, 0); /* kma.cl:343 */
+		uint32_t slots = st_slots(st);
+		uint32_t fr = st_free(st) + 1;
+		bool enq = fr == slots;
+		uint32_t nst = st_make(st_class(st), slots, enq ? 0 : fr);
+		if (cas_acqrel(stp, st, nst) == st) {
+			if (enq)
+				sb_recycle(h, s, c);
+			return;
+		}
+	}
+	set_err(h, KMA_ERR_TIMEOUT);
+}
+
+/* ------------------------------------------------------------------ */
+/* warp-collaborative malloc/free                                      */
+/* ------------------------------------------------------------------ */
+/* Lanes are grouped by size class with __match_any_sync.  The group   */
+/* leader reserves k slots with one CAS on the current superblock's     */
+/* state word (refilling from the free list when needed), then claims   */
+/* the bitmap bits one word at a time with one atomicOr per word; the   */
+/* claimed (superblock, word, mask) is broadcast with __shfl_sync and   */
+/* each lane picks its bit by rank.  One atomic per warp per superblock */
+/* (and per bitmap word) reaches L2 instead of two or three per lane.   */
+/* A single calling lane follows exactly the plain path's choices.      */
+/* ------------------------------------------------------------------ */
+namespace kma_detail {
+
+struct warp_claim {
+	uint32_t sb;     /* superblock index */
+	uint32_t word;   /* bitmap word index */
+	uint32_t got;    /* bits claimed in that word */
+	uint32_t base;   /* rank of the first lane served by this claim */
+	uint32_t hint;   /* hint of that first lane (word 0 of its block) */
+};
+
+/* Leader-side state of one group's reservation. */
+struct warp_resv {
+	uint32_t sb, cls, left, cursor, pre_hi, hint;
+	bool pre;
+};
+
+/* Reserve up to `want` slots of class c.  On success fills r (sb, left =
+ * number reserved, cursor = first slot to scan from, hint) and returns 1;
+ * returns 0 when the heap is exhausted or a spin expired. */
+__device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t want, warp_resv &r)
+{
+	uint32_t *clsw = &h->cls[c].v;
+	uint32_t lim = h->spin_limit;
+	for (uint32_t it = 0; it < lim; it++) {
+		uint32_t cur = ld_acquire(clsw);
+		if (cur == 0) {
+			if (cas_acqrel(clsw, 0, KMA_POISON) != 0)
+				continue;
+			int64_t s = sb_dequeue(h);
+			if (s < 0) {
+				atomicExch(clsw, 0);
+				return 0;
+			}
+			uint32_t slots = h->cls_slots[c];
+			uint32_t t = want < slots ? want : slots;
+			sb_format(h, (uint32_t)s, c, slots - t, slots - t);
+			/* the refiller takes the top t slots, which are exactly the
+			 * hints slots-1 .. slots-t of t serial reservations */
+			cas_acqrel(clsw, KMA_POISON, t == slots ? 0u : (uint32_t)s + KMA_CLS_BASE);
+			r.sb = (uint32_t)s;
+			r.cls = c;
+			r.left = t;
+			r.cursor = slots - t;
+			r.pre_hi = slots;
+			r.hint = slots - 1;
+			r.pre = true;
+			return 1;
+		}
+		if (cur == KMA_POISON) {
+			backoff(it);
+			continue;
+		}
+		uint32_t s = cur - KMA_CLS_BASE;
+		uint32_t *stp = &h->sb_state[s];
+		uint32_t st = ld_relaxed(stp);
+		if (st_class(st) != c || st_free(st) == 0) {
+			backoff(it);
+			continue;
+		}
+		uint32_t fr = st_free(st);
+		uint32_t t = want < fr ? want : fr;
+		if (cas_acqrel(stp, st, st - t) != st)
+			continue;
+		if (fr == t)
+			cas_acqrel(clsw, cur, 0);
+		r.sb = s;
+		r.cls = c;
+		r.left = t;
+		r.cursor = fr - t; /* lowest of the t serial hints fr-1 .. fr-t */
+		r.pre = false;
+		r.hint = fr - 1;
+		return 1;
+	}
+	set_err(h, KMA_ERR_TIMEOUT);
+	return 0;
+}
+
+/* One claim step on the reservation: claims bits in one bitmap word.
+ * Returns the claimed mask (possibly 0 when another thread won the bits
+ * and the word must be re-read), and the word index in `word`. */
+__device__ __forceinline__ uint32_t warp_claim_step(kma_heap *h, warp_resv &r, uint32_t &word)
+{
+	uint32_t slots = h->cls_slots[r.cls];
+	uint32_t k = r.cursor >> 5;
+	word = k;
+	uint32_t lo = r.cursor & 31;
+	if (r.pre) {
+		/* bits [cursor, pre_hi) were set by sb_format */
+		uint32_t hi = r.pre_hi < (k + 1) * 32 ? r.pre_hi - k * 32 : 32;
+		uint32_t n = hi - lo;
+		uint32_t got = (n == 32 ? 0xffffffffu : ((1u << n) - 1u)) << lo;
+		r.cursor = k * 32 + hi;
+		r.left -= n;
+		return got;
+	}
+	unsigned char *sb = h->sb_base + ((size_t)r.sb << h->sb_log2);
+	uint32_t *wp = bitmap_word(h, sb, k);
+	uint32_t words = h->cls_words[r.cls];
+	uint32_t valid = (k == words - 1 && (slots & 31)) ? ((1u << (slots & 31)) - 1u) : 0xffffffffu;
+	uint32_t v = ld_relaxed(wp);
+	uint32_t cand = ~v & valid & (0xffffffffu << lo);
+	uint32_t pick = 0;
+	/* take the lowest `left` candidate bits */
+	if (__popc(cand) <= (int)r.left) {
+		pick = cand;
+	} else {
+		uint32_t top = nth_set_bit(cand, r.left - 1);
+		pick = cand & (top == 31 ? 0xffffffffu : ((2u << top) - 1u));
+	}
+	uint32_t got = 0;
+	if (pick) {
+		uint32_t old = or_acqrel(wp, pick);
+		got = pick & ~old;
+	}
+	r.left -= __popc(got);
+	if (got == pick) {
+		/* every candidate we wanted is ours: move on if more are needed */
+		if (r.left && __popc(cand) <= __popc(pick)) {
+			r.cursor = (k + 1) * 32;
+			if (r.cursor >= slots)
+				r.cursor = 0;
+		}
+	}
+	return got;
+}
+
+} /* namespace kma_detail */
+
+__device__ inline void *kma_malloc_warp(kma_heap *h, size_t size)
+{
+	using namespace kma_detail;
+	const uint32_t active = __activemask();
+	const uint32_t lane = lane_id();
+	int c = kma_class_of(h, size);
+	uint32_t peers = __match_any_sync(active, c);
+	uint32_t leader = __ffs(peers) - 1;
+	uint32_t rank = __popc(peers & lanemask_lt());
+	uint32_t gsize = __popc(peers);
+	bool need = c >= 0;
+	void *res = NULL;
+
+	/* leader-only state */
+	warp_resv r;
+	r.left = 0;
+	uint32_t served = 0;
+	bool failed = false;
+	uint32_t guard = 0;
+	const uint32_t lim = h->spin_limit;
+
+	while (__any_sync(active, need)) {
+		uint32_t bsb = 0, bword = 0, bgot = 0, bbase = 0, bhint = 0, bfail = 0;
+		if (lane == leader && need && !failed) {
+			if (r.left == 0) {
+				if (!warp_reserve(h, (uint32_t)c, gsize - served, r))
+					failed = true;
+			}
+			if (!failed) {
+				uint32_t w;
+				uint32_t hint0 = r.hint;
+				uint32_t got = warp_claim_step(h, r, w);
+				bsb = r.sb;
+				bword = w;
+				bgot = got;
+				bbase = served;
+				bhint = hint0;
+				served += __popc(got);
+				r.hint -= __popc(got);
+				if (++guard > lim) {
+					set_err(h, KMA_ERR_TIMEOUT);
+					failed = true;
+				}
+			}
+			bfail = failed;
+		}
+		bsb = __shfl_sync(active, bsb, leader);
+		bword = __shfl_sync(active, bword, leader);
+		bgot = __shfl_sync(active, bgot, leader);
+		bbase = __shfl_sync(active, bbase, leader);
+		bhint = __shfl_sync(active, bhint, leader);
+		bfail = __shfl_sync(active, bfail, leader);
+		if (need) {
+			uint32_t n = __popc(bgot);
+			if (rank >= bbase && rank < bbase + n) {
+				/* rank j of this claim takes the j-th highest claimed bit,
+				 * matching the serial hint order fr-1, fr-2, ... */
+				uint32_t j = rank - bbase;
+				uint32_t b = nth_set_bit(bgot, n - 1 - j);
+				uint32_t slot = bword * 32 + b;
+				unsigned char *sb = h->sb_base + ((size_t)bsb << h->sb_log2);
+				unsigned char *p = sb + KMA_SB_HDR + (size_t)slot * h->cls_size[c];
+				*reinterpret_cast<uint32_t *>(p) = bhint - j;
+				res = p;
+				need = false;
+			} else if (bfail) {
+				need = false;
+			}
+		}
+	}
+	return res;
+}
+
+__device__ inline void kma_free_warp(kma_heap *h, void *p)
+{
+	using namespace kma_detail;
+	const uint32_t active = __activemask();
+	const uint32_t lane = lane_id();
+	uint32_t s = 0xffffffffu, c = 0, slot = 0;
+	bool valid = false;
+	if (p != NULL) {
+		valid = block_locate(h, p, s, c, slot);
+		if (!valid)
+			set_err(h, KMA_ERR_BADFREE);
+	}
+	/* 1) clear bitmap bits: one atomicAnd per (superblock, word) */
+	uint32_t word = valid ? (slot >> 5) : 0xffffffffu;
+	unsigned long long key = ((unsigned long long)s << 32) | word;
+	uint32_t wpeers = __match_any_sync(active, key);
+	uint32_t bit = valid ? (1u << (slot & 31)) : 0u;
+	uint32_t mask = __reduce_or_sync(wpeers, bit);
+	uint32_t wleader = __ffs(wpeers) - 1;
+	uint32_t old = 0;
+	if (valid && lane == wleader) {
+		unsigned char *sb = h->sb_base + ((size_t)s << h->sb_log2);
+		old = and_acqrel(bitmap_word(h, sb, word), ~mask);
+	}
+	old = __shfl_sync(active, old, wleader);
+	bool good = valid && (old & bit);
+	if (valid) {
+		*reinterpret_cast<volatile uint32_t *>(p) = old; /* kma.cl:338 */
+		if (!good)
+			set_err(h, KMA_ERR_BADFREE); /* double free, see kma_free */
+	}
+	/* 2) return k slots to the superblock: one state update per superblock */
+	uint32_t speers = __match_any_sync(active, good ? s : 0xffffffffu);
+	uint32_t k = __popc(speers);
+	uint32_t sleader = __ffs(speers) - 1;
+	if (good && lane == sleader) {
+		uint32_t *stp = &h->sb_state[s];
+		uint32_t lim = h->spin_limit;
+		uint32_t st = ld_relaxed(stp);
+		for (uint32_t it = 0; it < lim; it++) {
+			uint32_t slots = st_slots(st);
+			uint32_t fr = st_free(st) + k;
+			bool enq = fr == slots;
+			uint32_t nst = st_make(st_class(st), slots, enq ? 0 : fr);
+			uint32_t seen = cas_acqrel(stp, st, nst);
+			if (seen == st) {
+				if (enq)
+					sb_recycle(h, s, c);
+				return;
+			}
+			st = seen;
+		}
+		set_err(h, KMA_ERR_TIMEOUT);
+	}
+}
+
+#endif /* KMA_DEVICE_CUH */

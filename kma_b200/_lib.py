@@ -1,0 +1,125 @@
+"""ctypes binding of libkma_b200.so (the C ABI of include/kma.h).
+
+Loading never falls back to anything: if the library is missing or stale
+the import raises, and every compute call goes through the CUDA library.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import (POINTER, Structure, c_char_p, c_float, c_int, c_int32, c_int64, c_uint,
+                    c_uint32, c_uint64, c_void_p)
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libkma_b200.so")
+
+KMA_OK = 0
+KMA_EINVAL = -1
+KMA_ENOMEM = -2
+KMA_ECUDA = -3
+KMA_ETIMEDOUT = -4
+KMA_ENODEV = -5
+KMA_EFAULT = -6
+
+KMA_FLAG_TIMEOUT = 1
+KMA_FLAG_BADFREE = 2
+
+MODE_PLAIN = 0
+MODE_WARP = 1
+
+WL_C1 = 1
+WL_C2 = 2
+WL_CAP = 32
+
+
+class KmaError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        super().__init__(f"{what}: {strerror(code)} ({code})")
+
+
+class KmaConfig(Structure):
+    _fields_ = [("sblocks", c_uint32), ("sb_size_log2", c_uint32),
+                ("spin_limit", c_uint32), ("device", c_int32)]
+
+
+class KmaInfo(Structure):
+    _fields_ = [("region_bytes", c_uint64), ("device_bytes", c_uint64),
+                ("sblocks", c_uint32), ("pages", c_uint32), ("sb_size_log2", c_uint32),
+                ("nclasses", c_uint32), ("max_request", c_uint32),
+                ("cls_size", c_uint32 * 16), ("cls_slots", c_uint32 * 16)]
+
+
+class KmaWlStats(Structure):
+    _fields_ = [("mallocs", c_uint64), ("frees", c_uint64), ("nulls", c_uint64),
+                ("bad_tags", c_uint64), ("offset_hash", c_uint64), ("fill_bytes", c_uint64),
+                ("verify_bytes", c_uint64)]
+
+
+# (name, restype, argtypes) for every symbol include/kma.h declares
+SIGNATURES = [
+    ("kma_size_by_sbid", c_uint32, [c_uint32, c_int]),
+    ("kma_slots_by_size", c_int, [c_uint32, c_uint64]),
+    ("kma_sbid_by_size", c_int, [c_uint32, c_uint64]),
+    ("kma_create", c_void_p, [c_int, c_void_p, c_uint]),
+    ("kma_create_ex", c_int, [POINTER(KmaConfig), c_void_p, POINTER(c_void_p)]),
+    ("kma_destroy", c_int, [c_void_p]),
+    ("kma_reset", c_int, [c_void_p, c_void_p]),
+    ("kma_heap_device_ptr", c_void_p, [c_void_p]),
+    ("kma_get_info", c_int, [c_void_p, POINTER(KmaInfo)]),
+    ("kma_error_flags", c_int, [c_void_p, c_void_p, POINTER(c_uint32), c_int]),
+    ("kma_strerror", c_char_p, [c_int]),
+    ("kma_version", c_char_p, []),
+    ("kma_snapshot", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                             c_uint64, c_uint64, c_void_p]),
+    ("kma_gather_bitmaps", c_int, [c_void_p, c_void_p, c_void_p, c_uint32]),
+    ("kma_replay", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int, c_void_p]),
+    ("kma_replay_host", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int]),
+    ("kma_wl_create", c_int, [c_void_p, c_int, c_uint64, POINTER(c_void_p)]),
+    ("kma_wl_destroy", c_int, [c_void_p]),
+    ("kma_wl_begin", c_int, [c_void_p, c_uint64, c_void_p]),
+    ("kma_wl_begin_seeds", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("kma_wl_rounds", c_int, [c_void_p, c_uint32, c_int, c_uint32, c_void_p]),
+    ("kma_wl_drain", c_int, [c_void_p, c_int, c_uint32, c_void_p]),
+    ("kma_wl_serial", c_int, [c_void_p, c_uint32, c_int, c_int, c_void_p]),
+    ("kma_wl_run_host", c_int, [c_void_p, c_void_p, c_uint32, c_int, c_void_p,
+                                POINTER(KmaWlStats), c_void_p]),
+    ("kma_wl_stats_get", c_int, [c_void_p, c_void_p, POINTER(KmaWlStats)]),
+    ("kma_wl_item_hashes", c_void_p, [c_void_p]),
+    ("kma_wl_live", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("kma_debug_set_class_word", c_int, [c_void_p, c_uint32, c_uint32, c_void_p]),
+    ("kma_bench_atomics", c_int, [c_int, c_uint64, c_uint32, c_uint32, c_void_p, POINTER(c_float)]),
+]
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libkma_b200.so (building it first if the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    from . import build as _build
+    if _build.stale():
+        _build.build()
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run python -m kma_b200.build")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def strerror(code: int) -> str:
+    try:
+        return lib().kma_strerror(code).decode()
+    except Exception:  # noqa: BLE001 - only used to format an error
+        return "error"
+
+
+def check(code: int, what: str) -> None:
+    if code != KMA_OK:
+        raise KmaError(code, what)

@@ -1,0 +1,431 @@
+/*
+ * kma_heap.cu -- heap lifetime, bulk init/reset, snapshot and serial replay
+ * (C ABI of include/kma.h).
+ *
+ * Replaces kma.c:31-127 (kma_create: buffer + one-work-item clheap_init)
+ * and kma.cl:27-52 (clheap_init: empty class table, then pages-1 serial
+ * idxd_enqueue calls).  Here the free list is written directly as the
+ * pre-linked array those enqueues produce (superblock 0 the dummy, then
+ * 1..pages-1 in order), by a grid-stride kernel with 16-byte stores.
+ */
+#include <string.h>
+#include <stdlib.h>
+#include "kma_internal.h"
+
+/* ------------------------------------------------------------------ */
+/* class tables                                                        */
+/* ------------------------------------------------------------------ */
+
+/* kma.cl:55-90 */
+extern "C" uint32_t kma_size_by_sbid(uint32_t sb_log2, int block)
+{
+	if (sb_log2 < 4 || sb_log2 > 30)
+		return 0;
+	int buckets = (int)sb_log2 - 1;
+	uint64_t sbsz = 1ull << sb_log2;
+	/* kma.cl:61 admits block == buckets, which divides by zero at :87 */
+	if (block >= buckets || block < 0)
+		return 0;
+	block += 2;
+	if (block <= (int)(sb_log2 >> 1))
+		return 1u << block;
+	uint64_t bytes = 1ull << block;
+	uint64_t items = sbsz / bytes;
+	uint64_t alloc_bytes = items >> 3;
+	alloc_bytes += (items & 0x7) ? 1 : 0;
+	alloc_bytes += (alloc_bytes & 0x3) ? (4 - (alloc_bytes & 0x3)) : 0;
+	uint64_t total = sbsz - (12 + alloc_bytes);
+	uint64_t size = total / items;
+	return (uint32_t)(size & ~0x3ull);
+}
+
+/* kma.cl:95-113 */
+extern "C" int kma_slots_by_size(uint32_t sb_log2, uint64_t size)
+{
+	if (size == 0 || sb_log2 < 4 || sb_log2 > 30)
+		return 0;
+	uint64_t space = (1ull << sb_log2) - 12;
+	int64_t slots = (int64_t)(space / size);
+	if (slots & 0x1f)
+		slots += 32;
+	slots >>= 3;
+	slots &= ~0x3;
+	space -= (uint64_t)slots;
+	return (int)(space / size);
+}
+
+/* kma.cl:119-148.  The reference approximates the class from the MSB of
+ * size/4 and only ever walks upward from there, so it returns the
+ * smallest class whose block size is >= size; -1 above SB-16. */
+extern "C" int kma_sbid_by_size(uint32_t sb_log2, uint64_t size)
+{
+	if (sb_log2 < 4 || sb_log2 > 30)
+		return -1;
+	if (size > (1ull << sb_log2) - 16)
+		return -1;
+	int buckets = (int)sb_log2 - 1;
+	for (int c = 0; c < buckets; c++)
+		if (kma_size_by_sbid(sb_log2, c) >= size)
+			return c;
+	return -1;
+}
+
+int kma_fill_class_tables(uint32_t sb_log2, kma_heap *hh)
+{
+	uint32_t n = sb_log2 - 1;
+	if (n > KMA_MAX_CLASSES)
+		return KMA_EINVAL;
+	hh->nclasses = n;
+	hh->max_request = (1u << sb_log2) - 16;
+	for (uint32_t c = 0; c < KMA_MAX_CLASSES; c++) {
+		uint32_t sz = c < n ? kma_size_by_sbid(sb_log2, (int)c) : 0;
+		uint32_t sl = sz ? (uint32_t)kma_slots_by_size(sb_log2, sz) : 0;
+		hh->cls_size[c] = sz;
+		hh->cls_slots[c] = sl;
+		hh->cls_magic[c] = sz ? (uint32_t)((1ull << 32) / sz + 1) : 0;
+		hh->cls_words[c] = (sl + 31) / 32;
+		if (sl > KMA_ST_FREE_MASK)
+			return KMA_EINVAL;
+	}
+	if (hh->cls_size[n - 1] != hh->max_request)
+		return KMA_EINVAL;
+	return KMA_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* kernels                                                             */
+/* ------------------------------------------------------------------ */
+
+/* Bulk (re)initialisation: sb_state[] = 0, sb_next[] = the linked list
+ * 0 -> 1 -> ... -> pages-1, head = dummy 0, tail = pages-1, class table
+ * empty, error flags clear.  Four superblocks per thread, vector stores. */
+__global__ void kma_k_reset(kma_heap *h, uint32_t nsb, uint32_t pages)
+{
+	using namespace kma_detail;
+	uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	uint32_t *state = h->sb_state;
+	unsigned long long *next = h->sb_next;
+	uint64_t nquad = nsb / 4;
+	for (uint64_t q = tid; q < nquad; q += stride) {
+		uint32_t s = (uint32_t)(q * 4);
+		reinterpret_cast<uint4 *>(state)[q] = make_uint4(0, 0, 0, 0);
+		unsigned long long l[4];
+#pragma unroll
+		for (int i = 0; i < 4; i++)
+			l[i] = (s + i + 1 < pages) ? tw_make(0, s + i + 2) : 0ull;
+		reinterpret_cast<ulonglong2 *>(next)[2 * q] = make_ulonglong2(l[0], l[1]);
+		reinterpret_cast<ulonglong2 *>(next)[2 * q + 1] = make_ulonglong2(l[2], l[3]);
+	}
+	for (uint64_t s = nquad * 4 + tid; s < nsb; s += stride) {
+		state[s] = 0;
+		next[s] = (s + 1 < pages) ? tw_make(0, (uint32_t)s + 2) : 0ull;
+	}
+	if (tid == 0) {
+		h->free_head.v = tw_make(0, 1);
+		h->free_tail.v = tw_make(0, pages > 1 ? pages : 1);
+		for (int c = 0; c < KMA_MAX_CLASSES; c++)
+			h->cls[c].v = 0;
+		h->err.v = 0;
+	}
+}
+
+__global__ void kma_k_gather_bitmaps(kma_heap *h, uint32_t *dst, uint32_t words)
+{
+	uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	uint64_t n = (uint64_t)h->nsb * words;
+	for (uint64_t i = tid; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+		uint32_t s = (uint32_t)(i / words), k = (uint32_t)(i % words);
+		unsigned char *sb = h->sb_base + ((size_t)s << h->sb_log2);
+		dst[i] = *kma_detail::bitmap_word(h, sb, k);
+	}
+}
+
+/* One thread replays the op stream (see kma_replay in kma.h). */
+__global__ void kma_k_replay(kma_heap *h, const int64_t *ops, int64_t n, int64_t *out, int mode)
+{
+	if (blockIdx.x != 0 || threadIdx.x != 0)
+		return;
+	for (int64_t i = 0; i < n; i++) {
+		int64_t kind = ops[2 * i], arg = ops[2 * i + 1];
+		if (kind == 0) {
+			size_t sz = arg < 0 ? (size_t)-1 : (size_t)arg;
+			void *p = mode == KMA_MODE_WARP ? kma_malloc_warp(h, sz) : kma_malloc(h, sz);
+			out[i] = p ? (int64_t)((unsigned char *)p - h->sb_base) : -1;
+		} else {
+			void *q = NULL;
+			if (arg >= 0 && arg < i && out[arg] >= 0)
+				q = h->sb_base + out[arg];
+			if (mode == KMA_MODE_WARP)
+				kma_free_warp(h, q);
+			else
+				kma_free(h, q);
+			out[i] = 0;
+		}
+	}
+}
+
+/* ------------------------------------------------------------------ */
+/* C ABI                                                               */
+/* ------------------------------------------------------------------ */
+
+static size_t kma_align_up(size_t x, size_t a) { return (x + a - 1) & ~(a - 1); }
+
+static int kma_launch_reset(kma_heap_s *k, cudaStream_t st)
+{
+	uint32_t nsb = k->hh.nsb;
+	uint64_t work = (nsb + 3) / 4;
+	uint32_t threads = 256;
+	uint64_t blocks = (work + threads - 1) / threads;
+	if (blocks > 148 * 16)
+		blocks = 148 * 16;
+	if (blocks == 0)
+		blocks = 1;
+	kma_k_reset<<<(unsigned)blocks, threads, 0, st>>>(k->dh, nsb, k->hh.pages);
+	KMA_CUDA(cudaGetLastError());
+	return KMA_OK;
+}
+
+extern "C" int kma_create_ex(const kma_config *cfg, void *stream, kma_heap_t *out)
+{
+	if (!cfg || !out)
+		return KMA_EINVAL;
+	*out = NULL;
+	if (cfg->sblocks == 0 || cfg->sb_size_log2 < 12 || cfg->sb_size_log2 > 16)
+		return KMA_EINVAL;
+	if (cfg->sblocks > 0x7fffffffu)
+		return KMA_EINVAL;
+	kma_device_guard g(cfg->device);
+	if (!g.ok)
+		return KMA_ENODEV;
+	int dev;
+	KMA_CUDA(cudaGetDevice(&dev));
+
+	kma_heap_s *k = (kma_heap_s *)calloc(1, sizeof(*k));
+	if (!k)
+		return KMA_ENOMEM;
+	k->device = dev;
+	memset(&k->hh, 0, sizeof(k->hh));
+	if (kma_fill_class_tables(cfg->sb_size_log2, &k->hh) != KMA_OK) {
+		free(k);
+		return KMA_EINVAL;
+	}
+	uint64_t nsb = cfg->sblocks;
+	size_t hdr = kma_align_up(sizeof(kma_heap), 4096);
+	size_t st_bytes = kma_align_up(nsb * 4, 4096);
+	size_t nx_bytes = kma_align_up(nsb * 8, 4096);
+	size_t region = (size_t)nsb << cfg->sb_size_log2;
+	size_t total = hdr + st_bytes + nx_bytes + region;
+	if (cudaMalloc(&k->dev_mem, total) != cudaSuccess) {
+		cudaGetLastError();
+		free(k);
+		return KMA_ENOMEM;
+	}
+	k->dev_bytes = total;
+	unsigned char *base = (unsigned char *)k->dev_mem;
+	k->dh = (kma_heap *)base;
+	k->hh.sb_state = (uint32_t *)(base + hdr);
+	k->hh.sb_next = (unsigned long long *)(base + hdr + st_bytes);
+	k->hh.sb_base = base + hdr + st_bytes + nx_bytes;
+	k->hh.region_bytes = region;
+	k->hh.sb_log2 = cfg->sb_size_log2;
+	k->hh.sb_size = 1u << cfg->sb_size_log2;
+	k->hh.nsb = (uint32_t)nsb;
+	/* kma.cl:42: pages = (bytes >> LOG2) - 1 where bytes also counts the
+	 * header, i.e. sblocks - 1 superblocks enter the free list */
+	k->hh.pages = (uint32_t)nsb - 1;
+	k->hh.spin_limit = cfg->spin_limit ? cfg->spin_limit : KMA_DEFAULT_SPIN;
+	k->hh.flags = 0;
+	cudaStream_t st = kma_stream(stream);
+	int rc = KMA_OK;
+	if (cudaMemcpyAsync(k->dh, &k->hh, sizeof(kma_heap), cudaMemcpyHostToDevice, st) != cudaSuccess)
+		rc = KMA_ECUDA;
+	if (rc == KMA_OK)
+		rc = kma_launch_reset(k, st);
+	if (rc == KMA_OK && cudaStreamSynchronize(st) != cudaSuccess)
+		rc = KMA_ECUDA;
+	if (rc != KMA_OK) {
+		cudaFree(k->dev_mem);
+		free(k);
+		return rc;
+	}
+	*out = k;
+	return KMA_OK;
+}
+
+extern "C" kma_heap_t kma_create(int device, void *stream, unsigned int sblocks)
+{
+	kma_config cfg;
+	kma_heap_t h = NULL;
+	if (sblocks == 0)
+		return NULL;
+	cfg.sblocks = sblocks;
+	cfg.sb_size_log2 = 12;
+	cfg.spin_limit = 0;
+	cfg.device = device;
+	if (kma_create_ex(&cfg, stream, &h) != KMA_OK)
+		return NULL;
+	return h;
+}
+
+extern "C" int kma_destroy(kma_heap_t h)
+{
+	if (!h)
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	cudaError_t e = cudaFree(h->dev_mem);
+	free(h);
+	return e == cudaSuccess ? KMA_OK : KMA_ECUDA;
+}
+
+extern "C" int kma_reset(kma_heap_t h, void *stream)
+{
+	if (!h)
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	return kma_launch_reset(h, kma_stream(stream));
+}
+
+extern "C" struct kma_heap *kma_heap_device_ptr(kma_heap_t h) { return h ? h->dh : NULL; }
+
+extern "C" int kma_get_info(kma_heap_t h, kma_info *o)
+{
+	if (!h || !o)
+		return KMA_EINVAL;
+	memset(o, 0, sizeof(*o));
+	o->region_bytes = h->hh.region_bytes;
+	o->device_bytes = h->dev_bytes;
+	o->sblocks = h->hh.nsb;
+	o->pages = h->hh.pages;
+	o->sb_size_log2 = h->hh.sb_log2;
+	o->nclasses = h->hh.nclasses;
+	o->max_request = h->hh.max_request;
+	for (int c = 0; c < 16; c++) {
+		o->cls_size[c] = h->hh.cls_size[c];
+		o->cls_slots[c] = h->hh.cls_slots[c];
+	}
+	return KMA_OK;
+}
+
+extern "C" int kma_error_flags(kma_heap_t h, void *stream, uint32_t *flags, int clear)
+{
+	if (!h || !flags)
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	cudaStream_t st = kma_stream(stream);
+	KMA_CUDA(cudaMemcpyAsync(flags, &h->dh->err.v, 4, cudaMemcpyDeviceToHost, st));
+	if (clear)
+		KMA_CUDA(cudaMemsetAsync(&h->dh->err.v, 0, 4, st));
+	KMA_CUDA(cudaStreamSynchronize(st));
+	return KMA_OK;
+}
+
+extern "C" const char *kma_strerror(int err)
+{
+	switch (err) {
+	case KMA_OK: return "ok";
+	case KMA_EINVAL: return "invalid argument";
+	case KMA_ENOMEM: return "out of device memory";
+	case KMA_ECUDA: return "CUDA error";
+	case KMA_ETIMEDOUT: return "bounded device wait expired";
+	case KMA_ENODEV: return "no such CUDA device";
+	case KMA_EFAULT: return "invariant check failed";
+	default: return "unknown error";
+	}
+}
+
+extern "C" const char *kma_version(void) { return "kma_b200 1.0 sm_100a"; }
+
+extern "C" int kma_snapshot(kma_heap_t h, void *stream, uint32_t *cls, uint64_t *headtail,
+		uint32_t *state, uint64_t *next, uint64_t region_off, uint64_t region_len,
+		void *region_dst)
+{
+	if (!h)
+		return KMA_EINVAL;
+	if (region_dst && (region_off > h->hh.region_bytes || region_len > h->hh.region_bytes - region_off))
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	cudaStream_t st = kma_stream(stream);
+	kma_heap tmp;
+	KMA_CUDA(cudaMemcpyAsync(&tmp, h->dh, sizeof(kma_heap), cudaMemcpyDeviceToHost, st));
+	if (state)
+		KMA_CUDA(cudaMemcpyAsync(state, h->hh.sb_state, (size_t)h->hh.nsb * 4, cudaMemcpyDeviceToHost, st));
+	if (next)
+		KMA_CUDA(cudaMemcpyAsync(next, h->hh.sb_next, (size_t)h->hh.nsb * 8, cudaMemcpyDeviceToHost, st));
+	if (region_dst && region_len)
+		KMA_CUDA(cudaMemcpyAsync(region_dst, h->hh.sb_base + region_off, region_len,
+				cudaMemcpyDeviceToHost, st));
+	KMA_CUDA(cudaStreamSynchronize(st));
+	if (cls)
+		for (int c = 0; c < 16; c++)
+			cls[c] = tmp.cls[c].v;
+	if (headtail) {
+		headtail[0] = tmp.free_head.v;
+		headtail[1] = tmp.free_tail.v;
+	}
+	return KMA_OK;
+}
+
+extern "C" int kma_gather_bitmaps(kma_heap_t h, void *stream, uint32_t *dst, uint32_t words)
+{
+	if (!h || !dst || words == 0)
+		return KMA_EINVAL;
+	if ((uint64_t)words * 4 > h->hh.sb_size)
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	kma_k_gather_bitmaps<<<148 * 8, 256, 0, kma_stream(stream)>>>(h->dh, dst, words);
+	KMA_CUDA(cudaGetLastError());
+	return KMA_OK;
+}
+
+extern "C" int kma_replay(kma_heap_t h, const int64_t *ops, int64_t n, int64_t *out, int mode,
+		void *stream)
+{
+	if (!h || n < 0 || (n && (!ops || !out)))
+		return KMA_EINVAL;
+	if (mode != KMA_MODE_PLAIN && mode != KMA_MODE_WARP)
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	if (n == 0)
+		return KMA_OK;
+	kma_k_replay<<<1, 1, 0, kma_stream(stream)>>>(h->dh, ops, n, out, mode);
+	KMA_CUDA(cudaGetLastError());
+	return KMA_OK;
+}
+
+extern "C" int kma_replay_host(kma_heap_t h, const int64_t *ops, int64_t n, int64_t *out, int mode)
+{
+	if (!h || n < 0 || (n && (!ops || !out)))
+		return KMA_EINVAL;
+	if (n == 0)
+		return KMA_OK;
+	kma_device_guard g(h->device);
+	int64_t *dops = NULL, *dout = NULL;
+	int rc = KMA_OK;
+	if (cudaMalloc(&dops, (size_t)n * 16) != cudaSuccess || cudaMalloc(&dout, (size_t)n * 8) != cudaSuccess) {
+		cudaGetLastError();
+		rc = KMA_ENOMEM;
+	}
+	if (rc == KMA_OK && cudaMemcpy(dops, ops, (size_t)n * 16, cudaMemcpyHostToDevice) != cudaSuccess)
+		rc = KMA_ECUDA;
+	if (rc == KMA_OK)
+		rc = kma_replay(h, dops, n, dout, mode, NULL);
+	if (rc == KMA_OK && cudaMemcpy(out, dout, (size_t)n * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+		rc = KMA_ECUDA;
+	if (dops)
+		cudaFree(dops);
+	if (dout)
+		cudaFree(dout);
+	return rc;
+}
+
+extern "C" int kma_debug_set_class_word(kma_heap_t h, uint32_t cls, uint32_t value, void *stream)
+{
+	if (!h || cls >= h->hh.nclasses)
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	static_assert(sizeof(uint32_t) == 4, "u32");
+	KMA_CUDA(cudaMemcpyAsync(&h->dh->cls[cls].v, &value, 4, cudaMemcpyHostToDevice, kma_stream(stream)));
+	KMA_CUDA(cudaStreamSynchronize(kma_stream(stream)));
+	return KMA_OK;
+}

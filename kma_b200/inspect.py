@@ -1,0 +1,174 @@
+"""Heap inspector: decode a heap image into the canonical form shared with
+the reference, and check heap invariants.
+
+Canonical form (implementation-neutral, what serial replay compares):
+  cls[c]       superblock attached to class c, -1 empty, -2 POISON
+  sb_size[s]   block size of superblock s (0 if never used)
+  sb_slots[s]  slots, sb_free[s] free count (kma.cl:180 packs slots<<16|free)
+  freelist     superblock indices from the head (the dummy) to the tail
+  region       superblock bytes with each superblock's first 12 bytes
+               masked (header fields live elsewhere here), i.e. the
+               bitmaps and the word-0 residue malloc/free leave in blocks
+               (kma.cl:265, kma.cl:338)
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+SB_HDR = 12
+FREE_MASK = 0x3FFF
+
+
+@dataclass
+class HeapImage:
+    sb_size_log2: int
+    sblocks: int
+    pages: int
+    nclasses: int
+    cls_size: list
+    cls_slots: list
+    cls_raw: np.ndarray
+    head: int
+    tail: int
+    state: np.ndarray
+    next: np.ndarray
+    region: np.ndarray | None = None
+
+
+@dataclass
+class Canonical:
+    cls: np.ndarray
+    sb_size: np.ndarray
+    sb_slots: np.ndarray
+    sb_free: np.ndarray
+    freelist: np.ndarray
+    region: np.ndarray | None = None
+    notes: list = field(default_factory=list)
+
+
+def decode(img: HeapImage) -> Canonical:
+    raw = img.cls_raw[: img.nclasses].astype(np.int64)
+    cls = np.where(raw == 0, -1, np.where(raw == 1, -2, raw - 2)).astype(np.int64)
+    st = img.state.astype(np.uint64)
+    cl = (st >> 28).astype(np.int64)
+    slots = ((st >> 14) & FREE_MASK).astype(np.uint32)
+    free = (st & FREE_MASK).astype(np.uint32)
+    sizes = np.asarray(img.cls_size + [0] * (16 - len(img.cls_size)), np.uint32)
+    size = np.where(st == 0, 0, sizes[np.clip(cl, 0, 15)]).astype(np.uint32)
+    fl = []
+    idx = int(img.head) & 0xFFFFFFFF
+    limit = img.sblocks + 1
+    nxt = img.next
+    while idx != 0:
+        if len(fl) > limit:
+            fl = None
+            break
+        fl.append(idx - 1)
+        idx = int(nxt[idx - 1]) & 0xFFFFFFFF
+    canon = Canonical(cls=cls, sb_size=size, sb_slots=slots, sb_free=free,
+                      freelist=np.asarray(fl if fl is not None else [-1], np.int64))
+    if fl is None:
+        canon.notes.append("free list does not terminate (cycle)")
+    if img.region is not None:
+        canon.region = mask_headers(img.region, img.sb_size_log2)
+    return canon
+
+
+def mask_headers(region: np.ndarray, sb_size_log2: int) -> np.ndarray:
+    """Zero the first 12 bytes of every superblock (a copy)."""
+    r = np.array(region, dtype=np.uint8, copy=True).reshape(-1, 1 << sb_size_log2)
+    r[:, :SB_HDR] = 0
+    return r.reshape(-1)
+
+
+def bitmap_words(region: np.ndarray, sb_size_log2: int, s: int, words: int) -> np.ndarray:
+    """Bitmap words 0..words-1 of superblock s (word k at u32 index SB/4-1-k)."""
+    sb = 1 << sb_size_log2
+    w = region[s * sb:(s + 1) * sb].view(np.uint32)
+    return w[::-1][:words].copy()
+
+
+def check_canonical_empty(img: HeapImage, bitmaps: np.ndarray | None = None) -> list[str]:
+    """The state every heap returns to once all blocks are freed: no class
+    attached, every page on the free list exactly once, every bitmap of a
+    used superblock clear (from img.region, or bitmaps[s, k] when given)."""
+    c = decode(img)
+    bad = []
+    if np.any(c.cls != -1):
+        bad.append(f"class table not empty: {c.cls.tolist()}")
+    fl = c.freelist
+    if c.notes:
+        bad += c.notes
+    elif len(fl) != max(img.pages, 1):
+        bad.append(f"free list holds {len(fl)} superblocks, expected {max(img.pages, 1)}")
+    if len(np.unique(fl)) != len(fl):
+        bad.append("free list holds a superblock twice")
+    if np.any(fl >= max(img.pages, 1)):
+        bad.append("free list holds a superblock beyond the pages")
+    used = np.nonzero(c.sb_slots)[0]
+    if np.any(c.sb_free[used] != 0):
+        bad.append("a recycled superblock has a non-zero free count")
+    if bitmaps is not None:
+        for s in used:
+            words = (int(c.sb_slots[s]) + 31) // 32
+            if np.any(bitmaps[s, :words]):
+                bad.append(f"superblock {s} bitmap not clear")
+                break
+    elif img.region is not None:
+        for s in used:
+            words = (int(c.sb_slots[s]) + 31) // 32
+            if np.any(bitmap_words(img.region, img.sb_size_log2, int(s), words)):
+                bad.append(f"superblock {s} bitmap not clear")
+                break
+    return bad
+
+
+def check_live_blocks(img: HeapImage, off: np.ndarray, size: np.ndarray,
+                      bitmaps: np.ndarray | None = None) -> dict:
+    """Invariants over a set of live blocks (offsets from the first
+    superblock, requested sizes): no two overlap, each lies inside the data
+    area of a superblock of a class at least as large as the request, on
+    that class's slot grid, 4-byte aligned, and (given bitmaps[s, k]) its
+    bit is set.  Returns violation counts (all zero when the heap is sound)."""
+    off = np.asarray(off, np.int64)
+    size = np.asarray(size, np.int64)
+    sb = 1 << img.sb_size_log2
+    res = {"blocks": int(len(off)), "overlap": 0, "out_of_bounds": 0, "misaligned": 0,
+           "off_grid": 0, "class_too_small": 0, "bit_clear": 0, "duplicate": 0}
+    if len(off) == 0:
+        return res
+    order = np.argsort(off, kind="stable")
+    o, z = off[order], size[order]
+    res["duplicate"] = int(np.sum(o[1:] == o[:-1]))
+    res["overlap"] = int(np.sum(o[:-1] + z[:-1] > o[1:]))
+    res["misaligned"] = int(np.sum(off % 4 != 0))
+    s = off // sb
+    inb = (off >= 0) & (s < img.sblocks)
+    res["out_of_bounds"] += int(np.sum(~inb))
+    s = np.where(inb, s, 0)
+    st = img.state[s].astype(np.int64)
+    cl = st >> 28
+    slots = (st >> 14) & FREE_MASK
+    sizes = np.asarray(img.cls_size + [0] * (16 - len(img.cls_size)), np.int64)
+    csize = sizes[np.clip(cl, 0, 15)]
+    within = off - s * sb - SB_HDR
+    ok_state = (st != 0) & (cl < img.nclasses)
+    res["out_of_bounds"] += int(np.sum(inb & (~ok_state | (within < 0))))
+    good = inb & ok_state & (within >= 0) & (csize > 0)
+    slot = np.where(good, within // np.where(csize > 0, csize, 1), 0)
+    res["off_grid"] = int(np.sum(good & (within % np.where(csize > 0, csize, 1) != 0)))
+    res["out_of_bounds"] += int(np.sum(good & (slot >= slots)))
+    res["out_of_bounds"] += int(np.sum(good & (within + size > slots * csize)))
+    res["class_too_small"] = int(np.sum(good & (csize < size)))
+    if bitmaps is not None:
+        words = bitmaps.shape[1]
+        k = np.clip(slot // 32, 0, words - 1)
+        bits = (bitmaps[s, k].astype(np.int64) >> (slot % 32)) & 1
+        res["bit_clear"] = int(np.sum(good & (bits == 0)))
+    return res
+
+
+def violations(res: dict) -> int:
+    return sum(v for k, v in res.items() if k != "blocks")

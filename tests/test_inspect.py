@@ -1,0 +1,86 @@
+"""The heap inspector's checkers, on images built from the oracle (the
+mistakes are planted in oracle-side data, on the CPU)."""
+import numpy as np
+
+from kma_b200 import inspect as ins
+from oracle import oracle
+from opstream import make_stream
+
+
+def image_from_port(p, sblocks, log2, ops, out):
+    d = p.decode()
+    sizes = oracle.port_tables(log2)[0]
+    st = np.zeros(sblocks, np.uint32)
+    for s in range(sblocks):
+        if d["sb_slots"][s]:
+            c = sizes.index(int(d["sb_size"][s]))
+            st[s] = (c << 28) | (int(d["sb_slots"][s]) << 14) | int(d["sb_free"][s])
+    cls = np.zeros(16, np.uint32)
+    for c, v in enumerate(d["cls"]):
+        cls[c] = 0 if v == -1 else 1 if v == -2 else v + 2
+    nxt = np.zeros(sblocks, np.uint64)
+    fl = d["freelist"]
+    for a, b in zip(fl[:-1], fl[1:]):
+        nxt[a] = b + 1
+    img = ins.HeapImage(log2, sblocks, sblocks - 1, log2 - 1, sizes,
+                        oracle.port_tables(log2)[1], cls, int(fl[0]) + 1, int(fl[-1]) + 1,
+                        st, nxt, p.region())
+    return img, d
+
+
+def live_set(ops, out):
+    freed = {int(a) for k, a in ops if k == 1 and a >= 0}
+    idx = [i for i, (k, a) in enumerate(ops) if k == 0 and out[i] >= 0 and i not in freed]
+    return out[idx], ops[idx, 1]
+
+
+def bitmaps_of(img):
+    words = (img.cls_slots[0] + 31) // 32
+    return np.stack([ins.bitmap_words(img.region, img.sb_size_log2, s, words)
+                     for s in range(img.sblocks)])
+
+
+def test_clean_live_set_has_no_violations():
+    ops = make_stream(5, 1200, 12)
+    with oracle.Port(64, 12) as p:
+        out = p.replay(ops)
+        img, _ = image_from_port(p, 64, 12, ops, out)
+    off, size = live_set(ops, out)
+    res = ins.check_live_blocks(img, off, size, bitmaps_of(img))
+    assert res["blocks"] > 50 and ins.violations(res) == 0, res
+
+
+def test_planted_faults_are_caught():
+    ops = make_stream(6, 1200, 12)
+    with oracle.Port(64, 12) as p:
+        out = p.replay(ops)
+        img, _ = image_from_port(p, 64, 12, ops, out)
+    off, size = live_set(ops, out)
+    bm = bitmaps_of(img)
+    o2 = off.copy()
+    o2[1] = o2[0] + 4  # overlaps block 0, off its slot grid
+    r = ins.check_live_blocks(img, o2, size, bm)
+    assert r["overlap"] >= 1 and r["off_grid"] >= 1
+    s2 = size.copy()
+    s2[0] = 5000  # request larger than any class
+    assert ins.check_live_blocks(img, off, s2, bm)["class_too_small"] >= 1
+    o3 = off.copy()
+    o3[0] = 64 * 4096 + 12  # past the last superblock
+    assert ins.check_live_blocks(img, o3, size, bm)["out_of_bounds"] >= 1
+    bm2 = bm.copy()
+    bm2[:] = 0  # every bit cleared
+    assert ins.check_live_blocks(img, off, size, bm2)["bit_clear"] == len(off)
+
+
+def test_canonical_empty_after_drain_and_not_before():
+    from opstream import drain_stream
+    ops = make_stream(8, 800, 12)
+    with oracle.Port(40, 12) as p:
+        out = p.replay(ops)
+        img, _ = image_from_port(p, 40, 12, ops, out)
+        assert ins.check_canonical_empty(img)  # blocks still live
+    full = drain_stream(ops)
+    with oracle.Port(40, 12) as p:
+        out = p.replay(full)
+        img, _ = image_from_port(p, 40, 12, full, out)
+        assert ins.check_canonical_empty(img) == []
