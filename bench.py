@@ -188,27 +188,27 @@ def run_ours(args) -> int:
 
     mode = MODE_WARP if args.mode == "warp" else MODE_PLAIN
     stream = torch.cuda.current_stream()
-    heap = Heap(SBLOCKS, SB_LOG2, stream=stream)
+    heap = Heap(SBLOCKS, SB_LOG2, stream=stream, compat=(mode == MODE_PLAIN))
     wl = Workload(heap, WL_C2, ITEMS)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    def step(m, ev=None):
+    def step(hp, w, m, ev=None):
         if ev:
             ev[0].record(stream)
-        heap.reset(stream)
-        wl.begin(SEED, stream)
+        hp.reset(stream)
+        w.begin(SEED, stream)
         if ev:
             ev[1].record(stream)
-        wl.rounds(ROUNDS, m, stream=stream)
+        w.rounds(ROUNDS, m, stream=stream)
         if ev:
             ev[2].record(stream)
-        wl.drain(m, stream=stream)
+        w.drain(m, stream=stream)
         if ev:
             ev[3].record(stream)
 
-    def timed(m, steps, warmup, sampler=None):
+    def timed(hp, w, m, steps, warmup, sampler=None):
         for _ in range(warmup):
-            step(m)
+            step(hp, w, m)
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
@@ -218,7 +218,7 @@ def run_ours(args) -> int:
             sampler.start()
         for k in range(steps):
             flush.zero_()  # > L2, outside the timed events
-            step(m, evs[k])
+            step(hp, w, m, evs[k])
         torch.cuda.synchronize()
         clocks = sampler.stop() if sampler else None
         if world > 1:
@@ -230,7 +230,7 @@ def run_ours(args) -> int:
     sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
                            if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit()
                            else local)
-    step_ms, rounds_ms, clocks = timed(mode, args.steps, args.warmup, sampler)
+    step_ms, rounds_ms, clocks = timed(heap, wl, mode, args.steps, args.warmup, sampler)
     st = wl.stats(stream)
     ops_step = st["mallocs"] + st["frees"]
     total_ms = sum(step_ms)
@@ -277,12 +277,20 @@ def run_ours(args) -> int:
         p_same = 148 * 256 * 16 / (at_same_ms / 1e3)
         op_rate = rounds_ops / mean_rounds_s
 
-        # plain per-thread kernel on the same GPU (the >=5x denominator)
-        plain = None
+        # plain per-thread kernel on the same GPU (the >=5x denominator):
+        # the reference's algorithm and structures (one class table,
+        # tagged-CAS MS-queue free list), and the same per-thread calls on
+        # the default (sharded, ticket-ring) heap
+        plain = plain_default = None
         if not args.no_plain and mode != MODE_PLAIN:
-            p_ms, _, _ = timed(MODE_PLAIN, 2, 1)
+            with Heap(SBLOCKS, SB_LOG2, stream=stream, compat=True) as hc, \
+                    Workload(hc, WL_C2, ITEMS) as wc:
+                p_ms, _, _ = timed(hc, wc, MODE_PLAIN, 2, 1)
+                st_p = wc.stats(stream)
+                plain = (st_p["mallocs"] + st_p["frees"]) / (statistics.mean(p_ms) / 1e3) / 1e6
+            p_ms, _, _ = timed(heap, wl, MODE_PLAIN, 2, 1)
             st_p = wl.stats(stream)
-            plain = (st_p["mallocs"] + st_p["frees"]) / (statistics.mean(p_ms) / 1e3) / 1e6
+            plain_default = (st_p["mallocs"] + st_p["frees"]) / (statistics.mean(p_ms) / 1e3) / 1e6
 
         # end to end through the host-buffer C ABI call (pinned seeds in,
         # per-item hashes + counters out)
@@ -333,6 +341,8 @@ def run_ours(args) -> int:
                              "steps, outside the timed events",
                        "parallelism": f"replicas x{world}",
                        "plain_mops": round(plain, 3) if plain else None,
+                       "plain_default_heap_mops": round(plain_default, 3) if plain_default else None,
+                       "shards": heap.nshards,
                        "warp_over_plain": round(value / world / plain, 2) if plain else None},
             "roofline": {"bound": "hbm", "kernel": "k_wl_rounds<warp>",
                          "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",

@@ -45,11 +45,18 @@ extern "C" {
 typedef struct kma_heap_s *kma_heap_t;
 struct kma_heap; /* device-side header, see kma_device.cuh */
 
+/* kma_config.flags */
+#define KMA_CFG_COMPAT 1u /* the reference's structures: one class table and the
+			   * tagged-CAS MS queue as the superblock free list */
+
 typedef struct kma_config {
 	uint32_t sblocks;      /* superblocks, as kma_create(..., sblocks) (kma.c:79) */
 	uint32_t sb_size_log2; /* 12..16: 4 KiB (the reference's KMA_SB_SIZE, kma.h:27) .. 64 KiB */
 	uint32_t spin_limit;   /* bound on every device spin; 0 = default (1<<22) */
 	int32_t device;        /* CUDA ordinal; -1 = current device */
+	uint32_t shards;       /* class-table shards (1..64), a thread uses smid % shards;
+				* 0 = default: min(64, max(1, (sblocks-1)/1024)); 1 with COMPAT */
+	uint32_t flags;        /* KMA_CFG_* */
 } kma_config;
 
 typedef struct kma_info {
@@ -59,6 +66,8 @@ typedef struct kma_info {
 	uint32_t max_request;    /* largest request served: SB - 16 (kma.cl:126) */
 	uint32_t cls_size[16];   /* block size per class (kma.cl:55-90) */
 	uint32_t cls_slots[16];  /* slots per superblock per class (kma.cl:95-113) */
+	uint32_t nshards;
+	uint32_t flags;          /* KMA_CFG_* in effect */
 } kma_info;
 
 /* ---- size-class tables: pure host functions, no GPU needed ---------- */
@@ -95,15 +104,17 @@ const char *kma_version(void);
 
 /* ---- heap image for checkers ------------------------------------------ */
 /* Copies to host (any NULL destination is skipped), synchronising stream:
- *   cls[16]   raw class-table words (0 empty, 1 POISON, s+2 superblock s)
- *   headtail[2] free-list head/tail tagged words {tag:32|idx+1:32}
- *   state[sblocks]  class<<28 | slots<<14 | free
- *   next[sblocks]   tagged free-list links
+ *   cls[nshards*16]  raw class-table words, shard-major (0 empty, 1 POISON,
+ *                    s+2 superblock s)
+ *   state[sblocks]   class<<28 | slots<<14 | free
+ *   freelist[sblocks], *freelist_len: the superblock free list in FIFO
+ *                    order, head (the next one handed out) first; length
+ *                    UINT64_MAX if the list does not end (a cycle)
  * region_off/len: bytes of the superblock region (offset from the first
  * superblock) copied to region_dst. */
-int kma_snapshot(kma_heap_t h, void *stream, uint32_t *cls, uint64_t *headtail,
-		uint32_t *state, uint64_t *next, uint64_t region_off, uint64_t region_len,
-		void *region_dst);
+int kma_snapshot(kma_heap_t h, void *stream, uint32_t *cls, uint32_t *state,
+		uint32_t *freelist, uint64_t *freelist_len, uint64_t region_off,
+		uint64_t region_len, void *region_dst);
 /* Gather the allocation bitmap of every superblock into dst
  * (sblocks x words u32, word k of superblock s at dst[s*words + k]),
  * words = ceil(slots of class 0 / 32).  Device pointer dst. */

@@ -8,22 +8,41 @@
  * different sizes per lane):
  *   void *kma_malloc_warp(kma_heap *heap, size_t size);
  *   void  kma_free_warp(kma_heap *heap, void *p);
- * and the lock-free structures (kma_structs.cuh): clqueue, clindexedqueue,
- * cltree, clarraylist, and the PMA bump heap (pma_malloc/pma_free).
+ * The lock-free structures (clqueue, clindexedqueue, cltree, clarraylist)
+ * and the PMA bump heap are in kma_structs.cuh.
  *
  * Heap layout in HBM (one cudaMalloc per heap, owned by kma_create):
- *   [kma_heap header | sb_state[nsb] u32 | sb_next[nsb] u64 | superblocks]
- *   superblock s at sb_base + s*SB: bytes [0,12) reserved (keeps every block
- *   offset identical to the reference's in-band 12-byte header, kma.h:71-78),
- *   blocks from +12, allocation bitmap at the tail growing downward
- *   (bitmap word k = slots 32k..32k+31 at u32 index SB/4-1-k, kma.cl:183-188).
- *   The superblock header fields live in coalesced side arrays instead:
- *   sb_state[s] = class<<28 | slots<<14 | free  (the reference packs
- *   slots<<16 | free, kma.cl:180; the class field is what makes a stale
- *   reservation detectable), sb_next[s] = tagged free-list link.
- * Class table cls[c] (kma.h:84): 0 empty, 1 POISON (refill in progress),
- * s+2 = superblock s is the current one for class c.  Each hot word sits on
- * its own 128-byte line.
+ *   [kma_heap header | sb_state[nsb] u32 | sb_home[nsb] u8 |
+ *    free-list words | superblocks]
+ *   Superblock s lives at sb_base + s*SB: bytes [0,12) are reserved so that
+ *   every block offset equals the reference's (its in-band 12-byte header,
+ *   kma.h:71-78); blocks start at +12; the allocation bitmap sits at the
+ *   tail and grows downward (bitmap word k = slots 32k..32k+31 at u32 index
+ *   SB/4-1-k, kma.cl:183-188).  The header fields live in coalesced side
+ *   arrays: sb_state[s] = class<<28 | slots<<14 | free (the reference packs
+ *   slots<<16 | free, kma.cl:180; the class field makes a stale reservation
+ *   detectable) and sb_home[s] = the shard whose class table holds s.
+ *
+ * Class table (kma.h:84): word cls[shard][c] is 0 (empty), 1 (POISON,
+ * refill in progress) or s+2 (superblock s is the current one for class c
+ * in that shard).  Every hot word sits on its own 128-byte line.  A thread
+ * uses shard smid % nshards; a heap with one shard is the reference's
+ * single table.
+ *
+ * Superblock free list, FIFO with the reference's order and its rule that
+ * one superblock always stays behind as the queue's dummy
+ * (clIndexedQueue.cl:254-290 returns the old dummy; the first superblock
+ * handed out is superblock 0):
+ *   KMA_HEAP_RING (default): a ticket ring -- fetch-and-add on the head and
+ *     tail tickets, one {seq:32 | sb:32} word per slot, an availability
+ *     count -- so concurrent refills do not retry CAS loops on one word;
+ *   otherwise: the Michael-Scott queue with a dummy node over superblock
+ *     indices, links in sb_next[] as 64-bit {tag:32 | idx+1:32} words
+ *     (ABA-safe), as the reference builds it (clIndexedQueue.cl:194-290).
+ *
+ * One-thread-at-a-time execution never observes POISON, a lost CAS or a
+ * second shard, so every configuration returns the reference's offsets
+ * under serial replay.
  *
  * Every spin (POISON wait, CAS retry, queue helpers) is bounded by
  * heap->spin_limit iterations; on expiry the call fails (NULL / 0), sets
@@ -36,6 +55,7 @@
 #include <stddef.h>
 
 #define KMA_MAX_CLASSES 16
+#define KMA_MAX_SHARDS 64
 #define KMA_SB_HDR 12u
 #define KMA_POISON 1u
 #define KMA_CLS_BASE 2u
@@ -43,6 +63,9 @@
 #define KMA_ST_FREE_MASK 0x3fffu
 #define KMA_ST_SLOTS_SHIFT 14
 #define KMA_ST_CLASS_SHIFT 28
+
+/* heap->flags */
+#define KMA_HEAP_RING 1u
 
 /* heap->err bits */
 #define KMA_ERR_TIMEOUT 1u
@@ -61,7 +84,9 @@ struct __align__(128) kma_heap {
 	/* geometry: written by kma_create, read-only afterwards */
 	unsigned char *sb_base;
 	uint32_t *sb_state;
-	unsigned long long *sb_next;
+	uint8_t *sb_home;
+	unsigned long long *sb_next; /* MS-queue links [nsb] (no KMA_HEAP_RING) */
+	unsigned long long *ring;    /* ring slots [ring_cap] (KMA_HEAP_RING) */
 	unsigned long long region_bytes; /* nsb << sb_log2 */
 	uint32_t sb_log2;
 	uint32_t sb_size;
@@ -71,15 +96,18 @@ struct __align__(128) kma_heap {
 	uint32_t max_request;/* SB - 16 (kma.cl:126) */
 	uint32_t spin_limit;
 	uint32_t flags;
+	uint32_t nshards;
+	uint32_t ring_cap;
 	uint32_t cls_size[KMA_MAX_CLASSES];  /* kma.cl:55-90 */
 	uint32_t cls_slots[KMA_MAX_CLASSES]; /* kma.cl:95-113 */
 	uint32_t cls_magic[KMA_MAX_CLASSES]; /* floor(2^32/size)+1: exact x/size for x < 2^16 */
 	uint32_t cls_words[KMA_MAX_CLASSES]; /* bitmap words = ceil(slots/32) */
 	/* hot words, one line each */
-	kma_line64 free_head;
-	kma_line64 free_tail;
-	kma_line32 cls[KMA_MAX_CLASSES];
+	kma_line64 free_head; /* MS-queue head, or ring head ticket */
+	kma_line64 free_tail; /* MS-queue tail, or ring tail ticket */
+	kma_line32 ring_avail;
 	kma_line32 err;
+	kma_line32 cls[KMA_MAX_SHARDS * KMA_MAX_CLASSES];
 };
 
 /* ------------------------------------------------------------------ */
@@ -104,10 +132,6 @@ __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long l
 	unsigned long long v;
 	asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
 	return v;
-}
-__device__ __forceinline__ void st_relaxed(uint32_t *p, uint32_t v)
-{
-	asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ void st_release(uint32_t *p, uint32_t v)
 {
@@ -139,6 +163,13 @@ __device__ __forceinline__ uint32_t add_acqrel(uint32_t *p, uint32_t v)
 		     : "=r"(old) : "l"(p), "r"(v) : "memory");
 	return old;
 }
+__device__ __forceinline__ unsigned long long add64_acqrel(unsigned long long *p, unsigned long long v)
+{
+	unsigned long long old;
+	asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;"
+		     : "=l"(old) : "l"(p), "l"(v) : "memory");
+	return old;
+}
 __device__ __forceinline__ uint32_t or_acqrel(uint32_t *p, uint32_t v)
 {
 	uint32_t old;
@@ -162,6 +193,12 @@ __device__ __forceinline__ uint32_t lane_id()
 	uint32_t l;
 	asm volatile("mov.u32 %0, %%laneid;" : "=r"(l));
 	return l;
+}
+__device__ __forceinline__ uint32_t sm_id()
+{
+	uint32_t s;
+	asm volatile("mov.u32 %0, %%smid;" : "=r"(s));
+	return s;
 }
 __device__ __forceinline__ uint32_t lanemask_lt()
 {
@@ -211,10 +248,23 @@ __device__ __forceinline__ unsigned long long tw_make(uint32_t tag, uint32_t idx
 	return ((unsigned long long)tag << 32) | idx;
 }
 
+__device__ __forceinline__ unsigned char *sb_addr(const kma_heap *h, uint32_t s)
+{
+	return h->sb_base + ((size_t)s << h->sb_log2);
+}
 /* bitmap word k of superblock sb (u32 index SB/4-1-k from the SB start) */
 __device__ __forceinline__ uint32_t *bitmap_word(const kma_heap *h, unsigned char *sb, uint32_t k)
 {
 	return reinterpret_cast<uint32_t *>(sb + h->sb_size) - 1 - k;
+}
+__device__ __forceinline__ uint32_t my_shard(const kma_heap *h)
+{
+	uint32_t n = h->nshards;
+	return n > 1 ? sm_id() % n : 0u;
+}
+__device__ __forceinline__ uint32_t *cls_word(kma_heap *h, uint32_t shard, uint32_t c)
+{
+	return &h->cls[shard * KMA_MAX_CLASSES + c].v;
 }
 
 } /* namespace kma_detail */
@@ -240,16 +290,13 @@ __device__ __forceinline__ int kma_class_of(const kma_heap *h, size_t size)
 }
 
 /* ------------------------------------------------------------------ */
-/* superblock free list: MS queue with a dummy node over superblock     */
-/* indices (clIndexedQueue.cl:194-290), links in sb_next[], 64-bit      */
-/* {tag:32|idx:32} words (ABA-safe).  Dequeue returns the OLD dummy, as */
-/* the reference does (clIndexedQueue.cl:282-289), so the first         */
-/* superblock handed out is superblock 0.                               */
+/* superblock free list                                                */
 /* ------------------------------------------------------------------ */
 namespace kma_detail {
 
-/* Enqueue superblock s.  Returns 1, or 0 on spin-limit expiry. */
-__device__ __forceinline__ int sb_enqueue(kma_heap *h, uint32_t s)
+/* MS queue (clIndexedQueue.cl:194-247 idxd_enqueue).  Returns 1, or 0 on
+ * spin-limit expiry. */
+__device__ __forceinline__ int msq_enqueue(kma_heap *h, uint32_t s)
 {
 	unsigned long long *link = &h->sb_next[s];
 	uint32_t idx = s + 1;
@@ -276,9 +323,9 @@ __device__ __forceinline__ int sb_enqueue(kma_heap *h, uint32_t s)
 	return 0;
 }
 
-/* Dequeue: returns the superblock index, or -1 when only the dummy is
- * left (empty), or -2 on spin-limit expiry. */
-__device__ __forceinline__ int64_t sb_dequeue(kma_heap *h)
+/* MS queue dequeue (clIndexedQueue.cl:249-290): the superblock index, -1
+ * when only the dummy is left, -2 on spin-limit expiry. */
+__device__ __forceinline__ int64_t msq_dequeue(kma_heap *h)
 {
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
@@ -300,14 +347,83 @@ __device__ __forceinline__ int64_t sb_dequeue(kma_heap *h)
 	return -2;
 }
 
-/* Prepare superblock s for class c: zero its bitmap except the bits in
- * [pre_lo, slots) which are pre-set (claimed by the refiller), then
- * publish state = (c, slots, free).  kma.cl:177-189, with the bitmap
- * written before the state becomes visible. */
-__device__ __forceinline__ void sb_format(kma_heap *h, uint32_t s, uint32_t c, uint32_t pre_lo,
-		uint32_t fr)
+/* Ticket ring.  Slot p % cap holds {seq:32 | sb:32}; seq == p+1 means
+ * "filled by the enqueue with ticket p", seq == p means "free for the
+ * enqueue with ticket p".  ring_avail counts completed enqueues not yet
+ * claimed by a dequeue; a dequeue needs two (one stays behind, as the
+ * reference's dummy does). */
+__device__ __forceinline__ int ring_enqueue(kma_heap *h, uint32_t s)
 {
-	unsigned char *sb = h->sb_base + ((size_t)s << h->sb_log2);
+	unsigned long long pos = add64_acqrel(&h->free_tail.v, 1ull);
+	unsigned long long *slot = &h->ring[pos % h->ring_cap];
+	uint32_t lim = h->spin_limit;
+	for (uint32_t it = 0; it < lim; it++) {
+		unsigned long long w = ld_acquire64(slot);
+		if ((uint32_t)(w >> 32) == (uint32_t)pos) {
+			st_release64(slot, ((unsigned long long)(uint32_t)(pos + 1) << 32) | s);
+			add_acqrel(&h->ring_avail.v, 1u);
+			return 1;
+		}
+		backoff(it);
+	}
+	set_err(h, KMA_ERR_TIMEOUT);
+	return 0;
+}
+
+__device__ __forceinline__ int64_t ring_dequeue(kma_heap *h)
+{
+	int32_t *avail = reinterpret_cast<int32_t *>(&h->ring_avail.v);
+	int32_t old = atomicSub(avail, 1);
+	if (old < 2) {
+		/* near empty: undo, then claim only a count that is really there */
+		atomicAdd(avail, 1);
+		int32_t a = (int32_t)ld_acquire(&h->ring_avail.v);
+		uint32_t lim = h->spin_limit, it = 0;
+		for (;;) {
+			if (a < 2)
+				return -1;
+			int32_t seen = (int32_t)cas_acqrel(&h->ring_avail.v, (uint32_t)a, (uint32_t)(a - 1));
+			if (seen == a)
+				break;
+			a = seen;
+			if (++it >= lim) {
+				set_err(h, KMA_ERR_TIMEOUT);
+				return -2;
+			}
+		}
+	}
+	unsigned long long pos = add64_acqrel(&h->free_head.v, 1ull);
+	unsigned long long *slot = &h->ring[pos % h->ring_cap];
+	uint32_t lim = h->spin_limit;
+	for (uint32_t it = 0; it < lim; it++) {
+		unsigned long long w = ld_acquire64(slot);
+		if ((uint32_t)(w >> 32) == (uint32_t)(pos + 1)) {
+			st_release64(slot, (unsigned long long)(uint32_t)(pos + h->ring_cap) << 32);
+			return (int64_t)(uint32_t)w;
+		}
+		backoff(it);
+	}
+	set_err(h, KMA_ERR_TIMEOUT);
+	return -2;
+}
+
+__device__ __forceinline__ int sb_enqueue(kma_heap *h, uint32_t s)
+{
+	return (h->flags & KMA_HEAP_RING) ? ring_enqueue(h, s) : msq_enqueue(h, s);
+}
+__device__ __forceinline__ int64_t sb_dequeue(kma_heap *h)
+{
+	return (h->flags & KMA_HEAP_RING) ? ring_dequeue(h) : msq_dequeue(h);
+}
+
+/* Prepare superblock s for class c: zero its bitmap except the bits in
+ * [pre_lo, slots), which are pre-set (claimed by the refiller), record its
+ * home shard, then publish state = (c, slots, free).  kma.cl:177-189, with
+ * the bitmap written before the state becomes visible. */
+__device__ __forceinline__ void sb_format(kma_heap *h, uint32_t s, uint32_t c, uint32_t pre_lo,
+		uint32_t fr, uint32_t shard)
+{
+	unsigned char *sb = sb_addr(h, s);
 	uint32_t slots = h->cls_slots[c];
 	uint32_t words = h->cls_words[c];
 	for (uint32_t k = 0; k < words; k++) {
@@ -323,6 +439,7 @@ __device__ __forceinline__ void sb_format(kma_heap *h, uint32_t s, uint32_t c, u
 		}
 		*bitmap_word(h, sb, k) = v;
 	}
+	h->sb_home[s] = (uint8_t)shard;
 	fence_acqrel();
 	st_release(&h->sb_state[s], st_make(c, slots, fr));
 }
@@ -346,7 +463,7 @@ namespace kma_detail {
  * write the hint into word 0 of the block. */
 __device__ __forceinline__ void *sb_get_block(kma_heap *h, uint32_t s, uint32_t c, uint32_t hint)
 {
-	unsigned char *sb = h->sb_base + ((size_t)s << h->sb_log2);
+	unsigned char *sb = sb_addr(h, s);
 	uint32_t slots = h->cls_slots[c];
 	uint32_t size = h->cls_size[c];
 	uint32_t words = h->cls_words[c];
@@ -387,7 +504,8 @@ __device__ inline void *kma_malloc(kma_heap *h, size_t size)
 	int c = kma_class_of(h, size);
 	if (c < 0)
 		return NULL;
-	uint32_t *clsw = &h->cls[c].v;
+	uint32_t shard = my_shard(h);
+	uint32_t *clsw = cls_word(h, shard, (uint32_t)c);
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
 		/* kma.cl:163: CAS 0 -> POISON doubles as the read of the slot */
@@ -400,7 +518,7 @@ __device__ inline void *kma_malloc(kma_heap *h, size_t size)
 				return NULL;
 			}
 			uint32_t slots = h->cls_slots[c];
-			sb_format(h, (uint32_t)s, c, slots, slots - 1);
+			sb_format(h, (uint32_t)s, c, slots, slots - 1, shard);
 			/* kma.cl:191 publishes the superblock even when the refill
 			 * took its only slot (1-slot classes); every later request
 			 * of that class then spins on a full superblock until the
@@ -452,7 +570,8 @@ __device__ __forceinline__ bool block_locate(const kma_heap *h, const void *p, u
  * free: kma.cl:362-367. */
 __device__ __forceinline__ void sb_recycle(kma_heap *h, uint32_t s, uint32_t c)
 {
-	cas_acqrel(&h->cls[c].v, s + KMA_CLS_BASE, 0);
+	uint32_t home = h->sb_home[s];
+	cas_acqrel(cls_word(h, home, c), s + KMA_CLS_BASE, 0);
 	sb_enqueue(h, s);
 }
 } /* namespace kma_detail */
@@ -468,7 +587,7 @@ __device__ inline void kma_free(kma_heap *h, void *p)
 		set_err(h, KMA_ERR_BADFREE);
 		return;
 	}
-	unsigned char *sb = h->sb_base + ((size_t)s << h->sb_log2);
+	unsigned char *sb = sb_addr(h, s);
 	uint32_t bit = 1u << (slot & 31);
 	/* kma.cl:336-338: the old bitmap word lands in word 0 of the block */
 	uint32_t old = and_acqrel(bitmap_word(h, sb, slot >> 5), ~bit);
@@ -501,22 +620,16 @@ __device__ inline void kma_free(kma_heap *h, void *p)
 /* ------------------------------------------------------------------ */
 /* Lanes are grouped by size class with __match_any_sync.  The group   */
 /* leader reserves k slots with one CAS on the current superblock's     */
-/* state word (refilling from the free list when needed), then claims   */
-/* the bitmap bits one word at a time with one atomicOr per word; the   */
-/* claimed (superblock, word, mask) is broadcast with __shfl_sync and   */
-/* each lane picks its bit by rank.  One atomic per warp per superblock */
-/* (and per bitmap word) reaches L2 instead of two or three per lane.   */
-/* A single calling lane follows exactly the plain path's choices.      */
+/* state word (refilling from the free list when needed; a group that   */
+/* needs a whole superblock takes a fresh one without touching the      */
+/* class table), then claims the bitmap bits one word at a time with    */
+/* one atomicOr per word; the claimed (superblock, word, mask) is       */
+/* broadcast with __shfl_sync and each lane picks its bit by rank.  One */
+/* atomic per warp per superblock (and per bitmap word) reaches L2      */
+/* instead of two or three per lane.  A single calling lane follows     */
+/* exactly the plain path's choices.                                    */
 /* ------------------------------------------------------------------ */
 namespace kma_detail {
-
-struct warp_claim {
-	uint32_t sb;     /* superblock index */
-	uint32_t word;   /* bitmap word index */
-	uint32_t got;    /* bits claimed in that word */
-	uint32_t base;   /* rank of the first lane served by this claim */
-	uint32_t hint;   /* hint of that first lane (word 0 of its block) */
-};
 
 /* Leader-side state of one group's reservation. */
 struct warp_resv {
@@ -529,7 +642,25 @@ struct warp_resv {
  * returns 0 when the heap is exhausted or a spin expired. */
 __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t want, warp_resv &r)
 {
-	uint32_t *clsw = &h->cls[c].v;
+	uint32_t slots = h->cls_slots[c];
+	uint32_t shard = my_shard(h);
+	if (want >= slots && slots > 1) {
+		/* the group fills a whole superblock: take a fresh one privately
+		 * (it would be detached at once anyway) */
+		int64_t s = sb_dequeue(h);
+		if (s < 0)
+			return 0;
+		sb_format(h, (uint32_t)s, c, 0, 0, shard);
+		r.sb = (uint32_t)s;
+		r.cls = c;
+		r.left = slots;
+		r.cursor = 0;
+		r.pre_hi = slots;
+		r.hint = slots - 1;
+		r.pre = true;
+		return 1;
+	}
+	uint32_t *clsw = cls_word(h, shard, c);
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
 		uint32_t cur = ld_acquire(clsw);
@@ -541,9 +672,8 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 				atomicExch(clsw, 0);
 				return 0;
 			}
-			uint32_t slots = h->cls_slots[c];
 			uint32_t t = want < slots ? want : slots;
-			sb_format(h, (uint32_t)s, c, slots - t, slots - t);
+			sb_format(h, (uint32_t)s, c, slots - t, slots - t, shard);
 			/* the refiller takes the top t slots, which are exactly the
 			 * hints slots-1 .. slots-t of t serial reservations */
 			cas_acqrel(clsw, KMA_POISON, t == slots ? 0u : (uint32_t)s + KMA_CLS_BASE);
@@ -603,7 +733,7 @@ __device__ __forceinline__ uint32_t warp_claim_step(kma_heap *h, warp_resv &r, u
 		r.left -= n;
 		return got;
 	}
-	unsigned char *sb = h->sb_base + ((size_t)r.sb << h->sb_log2);
+	unsigned char *sb = sb_addr(h, r.sb);
 	uint32_t *wp = bitmap_word(h, sb, k);
 	uint32_t words = h->cls_words[r.cls];
 	uint32_t valid = (k == words - 1 && (slots & 31)) ? ((1u << (slots & 31)) - 1u) : 0xffffffffu;
@@ -649,17 +779,26 @@ __device__ inline void *kma_malloc_warp(kma_heap *h, size_t size)
 	bool need = c >= 0;
 	void *res = NULL;
 
-	/* leader-only state */
+	/* leader-only state: the leader serves its whole group, not only itself */
 	warp_resv r;
 	r.left = 0;
 	uint32_t served = 0;
 	bool failed = false;
-	uint32_t guard = 0;
 	const uint32_t lim = h->spin_limit;
+	uint32_t rounds = 0;
 
 	while (__any_sync(active, need)) {
+		/* every lane runs every iteration, so this bound ends the loop for
+		 * all of them together */
+		if (++rounds > lim) {
+			if (need) {
+				need = false;
+				set_err(h, KMA_ERR_TIMEOUT);
+			}
+			continue;
+		}
 		uint32_t bsb = 0, bword = 0, bgot = 0, bbase = 0, bhint = 0, bfail = 0;
-		if (lane == leader && need && !failed) {
+		if (lane == leader && c >= 0 && served < gsize && !failed) {
 			if (r.left == 0) {
 				if (!warp_reserve(h, (uint32_t)c, gsize - served, r))
 					failed = true;
@@ -675,10 +814,6 @@ __device__ inline void *kma_malloc_warp(kma_heap *h, size_t size)
 				bhint = hint0;
 				served += __popc(got);
 				r.hint -= __popc(got);
-				if (++guard > lim) {
-					set_err(h, KMA_ERR_TIMEOUT);
-					failed = true;
-				}
 			}
 			bfail = failed;
 		}
@@ -696,8 +831,7 @@ __device__ inline void *kma_malloc_warp(kma_heap *h, size_t size)
 				uint32_t j = rank - bbase;
 				uint32_t b = nth_set_bit(bgot, n - 1 - j);
 				uint32_t slot = bword * 32 + b;
-				unsigned char *sb = h->sb_base + ((size_t)bsb << h->sb_log2);
-				unsigned char *p = sb + KMA_SB_HDR + (size_t)slot * h->cls_size[c];
+				unsigned char *p = sb_addr(h, bsb) + KMA_SB_HDR + (size_t)slot * h->cls_size[c];
 				*reinterpret_cast<uint32_t *>(p) = bhint - j;
 				res = p;
 				need = false;
@@ -729,10 +863,8 @@ __device__ inline void kma_free_warp(kma_heap *h, void *p)
 	uint32_t mask = __reduce_or_sync(wpeers, bit);
 	uint32_t wleader = __ffs(wpeers) - 1;
 	uint32_t old = 0;
-	if (valid && lane == wleader) {
-		unsigned char *sb = h->sb_base + ((size_t)s << h->sb_log2);
-		old = and_acqrel(bitmap_word(h, sb, word), ~mask);
-	}
+	if (valid && lane == wleader)
+		old = and_acqrel(bitmap_word(h, sb_addr(h, s), word), ~mask);
 	old = __shfl_sync(active, old, wleader);
 	bool good = valid && (old & bit);
 	if (valid) {

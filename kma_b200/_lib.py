@@ -38,16 +38,21 @@ class KmaError(RuntimeError):
         super().__init__(f"{what}: {strerror(code)} ({code})")
 
 
+KMA_CFG_COMPAT = 1
+
+
 class KmaConfig(Structure):
     _fields_ = [("sblocks", c_uint32), ("sb_size_log2", c_uint32),
-                ("spin_limit", c_uint32), ("device", c_int32)]
+                ("spin_limit", c_uint32), ("device", c_int32), ("shards", c_uint32),
+                ("flags", c_uint32)]
 
 
 class KmaInfo(Structure):
     _fields_ = [("region_bytes", c_uint64), ("device_bytes", c_uint64),
                 ("sblocks", c_uint32), ("pages", c_uint32), ("sb_size_log2", c_uint32),
                 ("nclasses", c_uint32), ("max_request", c_uint32),
-                ("cls_size", c_uint32 * 16), ("cls_slots", c_uint32 * 16)]
+                ("cls_size", c_uint32 * 16), ("cls_slots", c_uint32 * 16),
+                ("nshards", c_uint32), ("flags", c_uint32)]
 
 
 class KmaWlStats(Structure):

@@ -5,11 +5,12 @@
  * Replaces kma.c:31-127 (kma_create: buffer + one-work-item clheap_init)
  * and kma.cl:27-52 (clheap_init: empty class table, then pages-1 serial
  * idxd_enqueue calls).  Here the free list is written directly as the
- * pre-linked array those enqueues produce (superblock 0 the dummy, then
- * 1..pages-1 in order), by a grid-stride kernel with 16-byte stores.
+ * state those enqueues produce (superblock 0 at the head as the dummy,
+ * then 1..pages-1 in order) by a grid-stride kernel with 16-byte stores.
  */
 #include <string.h>
 #include <stdlib.h>
+#include <vector>
 #include "kma_internal.h"
 
 /* ------------------------------------------------------------------ */
@@ -96,36 +97,59 @@ int kma_fill_class_tables(uint32_t sb_log2, kma_heap *hh)
 /* kernels                                                             */
 /* ------------------------------------------------------------------ */
 
-/* Bulk (re)initialisation: sb_state[] = 0, sb_next[] = the linked list
- * 0 -> 1 -> ... -> pages-1, head = dummy 0, tail = pages-1, class table
- * empty, error flags clear.  Four superblocks per thread, vector stores. */
-__global__ void kma_k_reset(kma_heap *h, uint32_t nsb, uint32_t pages)
+/* Bulk (re)initialisation: sb_state[] = 0; the free list holds superblocks
+ * 0..n-1 in order (n = max(pages, 1): superblock 0 is the dummy even when
+ * no other page exists, kma.cl:48); class tables empty; flags clear.  Four
+ * superblocks per thread with 16-byte stores. */
+__global__ void kma_k_reset(kma_heap *h, uint32_t nsb, uint32_t nfree)
 {
 	using namespace kma_detail;
 	uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
 	uint32_t *state = h->sb_state;
-	unsigned long long *next = h->sb_next;
+	const bool ring = h->flags & KMA_HEAP_RING;
+	unsigned long long *w = ring ? h->ring : h->sb_next;
 	uint64_t nquad = nsb / 4;
-	for (uint64_t q = tid; q < nquad; q += stride) {
-		uint32_t s = (uint32_t)(q * 4);
+	for (uint64_t q = tid; q < nquad; q += stride)
 		reinterpret_cast<uint4 *>(state)[q] = make_uint4(0, 0, 0, 0);
-		unsigned long long l[4];
-#pragma unroll
-		for (int i = 0; i < 4; i++)
-			l[i] = (s + i + 1 < pages) ? tw_make(0, s + i + 2) : 0ull;
-		reinterpret_cast<ulonglong2 *>(next)[2 * q] = make_ulonglong2(l[0], l[1]);
-		reinterpret_cast<ulonglong2 *>(next)[2 * q + 1] = make_ulonglong2(l[2], l[3]);
-	}
-	for (uint64_t s = nquad * 4 + tid; s < nsb; s += stride) {
+	for (uint64_t s = nquad * 4 + tid; s < nsb; s += stride)
 		state[s] = 0;
-		next[s] = (s + 1 < pages) ? tw_make(0, (uint32_t)s + 2) : 0ull;
+	/* ring: slot i filled by ticket i ({seq i+1 | sb i}); MS queue: link
+	 * i -> i+1, the last link null */
+	uint64_t nw = ring ? h->ring_cap : nsb;
+	uint64_t npair = nw / 2;
+	for (uint64_t q = tid; q < npair; q += stride) {
+		unsigned long long l[2];
+#pragma unroll
+		for (int i = 0; i < 2; i++) {
+			uint32_t s = (uint32_t)(2 * q + i);
+			if (ring)
+				l[i] = s < nfree ? (((unsigned long long)(s + 1) << 32) | s)
+						 : ((unsigned long long)s << 32);
+			else
+				l[i] = (s + 1 < nfree) ? tw_make(0, s + 2) : 0ull;
+		}
+		reinterpret_cast<ulonglong2 *>(w)[q] = make_ulonglong2(l[0], l[1]);
 	}
+	for (uint64_t i = npair * 2 + tid; i < nw; i += stride) {
+		uint32_t s = (uint32_t)i;
+		if (ring)
+			w[i] = s < nfree ? (((unsigned long long)(s + 1) << 32) | s) : ((unsigned long long)s << 32);
+		else
+			w[i] = (s + 1 < nfree) ? tw_make(0, s + 2) : 0ull;
+	}
+	for (uint64_t i = tid; i < (uint64_t)KMA_MAX_SHARDS * KMA_MAX_CLASSES; i += stride)
+		h->cls[i].v = 0;
 	if (tid == 0) {
-		h->free_head.v = tw_make(0, 1);
-		h->free_tail.v = tw_make(0, pages > 1 ? pages : 1);
-		for (int c = 0; c < KMA_MAX_CLASSES; c++)
-			h->cls[c].v = 0;
+		if (ring) {
+			h->free_head.v = 0;
+			h->free_tail.v = nfree;
+			h->ring_avail.v = nfree;
+		} else {
+			h->free_head.v = tw_make(0, 1);
+			h->free_tail.v = tw_make(0, nfree);
+			h->ring_avail.v = 0;
+		}
 		h->err.v = 0;
 	}
 }
@@ -136,8 +160,7 @@ __global__ void kma_k_gather_bitmaps(kma_heap *h, uint32_t *dst, uint32_t words)
 	uint64_t n = (uint64_t)h->nsb * words;
 	for (uint64_t i = tid; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
 		uint32_t s = (uint32_t)(i / words), k = (uint32_t)(i % words);
-		unsigned char *sb = h->sb_base + ((size_t)s << h->sb_log2);
-		dst[i] = *kma_detail::bitmap_word(h, sb, k);
+		dst[i] = *kma_detail::bitmap_word(h, kma_detail::sb_addr(h, s), k);
 	}
 }
 
@@ -171,17 +194,18 @@ __global__ void kma_k_replay(kma_heap *h, const int64_t *ops, int64_t n, int64_t
 
 static size_t kma_align_up(size_t x, size_t a) { return (x + a - 1) & ~(a - 1); }
 
+static uint32_t kma_nfree(const kma_heap &hh) { return hh.pages > 1 ? hh.pages : 1; }
+
 static int kma_launch_reset(kma_heap_s *k, cudaStream_t st)
 {
-	uint32_t nsb = k->hh.nsb;
-	uint64_t work = (nsb + 3) / 4;
+	uint64_t work = ((uint64_t)k->hh.nsb + 3) / 4;
 	uint32_t threads = 256;
 	uint64_t blocks = (work + threads - 1) / threads;
+	if (blocks < 4)
+		blocks = 4; /* enough threads for the class-table lines */
 	if (blocks > 148 * 16)
 		blocks = 148 * 16;
-	if (blocks == 0)
-		blocks = 1;
-	kma_k_reset<<<(unsigned)blocks, threads, 0, st>>>(k->dh, nsb, k->hh.pages);
+	kma_k_reset<<<(unsigned)blocks, threads, 0, st>>>(k->dh, k->hh.nsb, kma_nfree(k->hh));
 	KMA_CUDA(cudaGetLastError());
 	return KMA_OK;
 }
@@ -193,7 +217,9 @@ extern "C" int kma_create_ex(const kma_config *cfg, void *stream, kma_heap_t *ou
 	*out = NULL;
 	if (cfg->sblocks == 0 || cfg->sb_size_log2 < 12 || cfg->sb_size_log2 > 16)
 		return KMA_EINVAL;
-	if (cfg->sblocks > 0x7fffffffu)
+	if (cfg->sblocks > 0x7fffffffu || cfg->shards > KMA_MAX_SHARDS)
+		return KMA_EINVAL;
+	if (cfg->flags & ~KMA_CFG_COMPAT)
 		return KMA_EINVAL;
 	kma_device_guard g(cfg->device);
 	if (!g.ok)
@@ -211,11 +237,27 @@ extern "C" int kma_create_ex(const kma_config *cfg, void *stream, kma_heap_t *ou
 		return KMA_EINVAL;
 	}
 	uint64_t nsb = cfg->sblocks;
+	/* kma.cl:42: pages = (bytes >> LOG2) - 1 where bytes also counts the
+	 * header, i.e. sblocks - 1 superblocks enter the free list */
+	k->hh.pages = (uint32_t)nsb - 1;
+	const bool compat = cfg->flags & KMA_CFG_COMPAT;
+	uint32_t shards = cfg->shards;
+	if (compat)
+		shards = 1;
+	else if (shards == 0) {
+		shards = k->hh.pages / 1024;
+		shards = shards < 1 ? 1 : shards > KMA_MAX_SHARDS ? KMA_MAX_SHARDS : shards;
+	}
+	k->hh.nshards = shards;
+	k->hh.flags = compat ? 0u : KMA_HEAP_RING;
+	k->hh.ring_cap = kma_nfree(k->hh);
+
 	size_t hdr = kma_align_up(sizeof(kma_heap), 4096);
 	size_t st_bytes = kma_align_up(nsb * 4, 4096);
-	size_t nx_bytes = kma_align_up(nsb * 8, 4096);
+	size_t home_bytes = kma_align_up(nsb, 4096);
+	size_t fl_bytes = kma_align_up((compat ? nsb : k->hh.ring_cap) * 8, 4096);
 	size_t region = (size_t)nsb << cfg->sb_size_log2;
-	size_t total = hdr + st_bytes + nx_bytes + region;
+	size_t total = hdr + st_bytes + home_bytes + fl_bytes + region;
 	if (cudaMalloc(&k->dev_mem, total) != cudaSuccess) {
 		cudaGetLastError();
 		free(k);
@@ -224,21 +266,27 @@ extern "C" int kma_create_ex(const kma_config *cfg, void *stream, kma_heap_t *ou
 	k->dev_bytes = total;
 	unsigned char *base = (unsigned char *)k->dev_mem;
 	k->dh = (kma_heap *)base;
-	k->hh.sb_state = (uint32_t *)(base + hdr);
-	k->hh.sb_next = (unsigned long long *)(base + hdr + st_bytes);
-	k->hh.sb_base = base + hdr + st_bytes + nx_bytes;
+	size_t o = hdr;
+	k->hh.sb_state = (uint32_t *)(base + o);
+	o += st_bytes;
+	k->hh.sb_home = (uint8_t *)(base + o);
+	o += home_bytes;
+	if (compat)
+		k->hh.sb_next = (unsigned long long *)(base + o);
+	else
+		k->hh.ring = (unsigned long long *)(base + o);
+	o += fl_bytes;
+	k->hh.sb_base = base + o;
 	k->hh.region_bytes = region;
 	k->hh.sb_log2 = cfg->sb_size_log2;
 	k->hh.sb_size = 1u << cfg->sb_size_log2;
 	k->hh.nsb = (uint32_t)nsb;
-	/* kma.cl:42: pages = (bytes >> LOG2) - 1 where bytes also counts the
-	 * header, i.e. sblocks - 1 superblocks enter the free list */
-	k->hh.pages = (uint32_t)nsb - 1;
 	k->hh.spin_limit = cfg->spin_limit ? cfg->spin_limit : KMA_DEFAULT_SPIN;
-	k->hh.flags = 0;
 	cudaStream_t st = kma_stream(stream);
 	int rc = KMA_OK;
-	if (cudaMemcpyAsync(k->dh, &k->hh, sizeof(kma_heap), cudaMemcpyHostToDevice, st) != cudaSuccess)
+	/* the geometry part of the header (everything before the hot lines) */
+	if (cudaMemcpyAsync(k->dh, &k->hh, offsetof(kma_heap, free_head), cudaMemcpyHostToDevice, st) !=
+			cudaSuccess)
 		rc = KMA_ECUDA;
 	if (rc == KMA_OK)
 		rc = kma_launch_reset(k, st);
@@ -259,9 +307,9 @@ extern "C" kma_heap_t kma_create(int device, void *stream, unsigned int sblocks)
 	kma_heap_t h = NULL;
 	if (sblocks == 0)
 		return NULL;
+	memset(&cfg, 0, sizeof(cfg));
 	cfg.sblocks = sblocks;
 	cfg.sb_size_log2 = 12;
-	cfg.spin_limit = 0;
 	cfg.device = device;
 	if (kma_create_ex(&cfg, stream, &h) != KMA_OK)
 		return NULL;
@@ -304,6 +352,8 @@ extern "C" int kma_get_info(kma_heap_t h, kma_info *o)
 		o->cls_size[c] = h->hh.cls_size[c];
 		o->cls_slots[c] = h->hh.cls_slots[c];
 	}
+	o->nshards = h->hh.nshards;
+	o->flags = (h->hh.flags & KMA_HEAP_RING) ? 0u : KMA_CFG_COMPAT;
 	return KMA_OK;
 }
 
@@ -334,10 +384,10 @@ extern "C" const char *kma_strerror(int err)
 	}
 }
 
-extern "C" const char *kma_version(void) { return "kma_b200 1.0 sm_100a"; }
+extern "C" const char *kma_version(void) { return "kma_b200 1.1 sm_100a"; }
 
-extern "C" int kma_snapshot(kma_heap_t h, void *stream, uint32_t *cls, uint64_t *headtail,
-		uint32_t *state, uint64_t *next, uint64_t region_off, uint64_t region_len,
+extern "C" int kma_snapshot(kma_heap_t h, void *stream, uint32_t *cls, uint32_t *state,
+		uint32_t *freelist, uint64_t *freelist_len, uint64_t region_off, uint64_t region_len,
 		void *region_dst)
 {
 	if (!h)
@@ -346,24 +396,58 @@ extern "C" int kma_snapshot(kma_heap_t h, void *stream, uint32_t *cls, uint64_t 
 		return KMA_EINVAL;
 	kma_device_guard g(h->device);
 	cudaStream_t st = kma_stream(stream);
-	kma_heap tmp;
-	KMA_CUDA(cudaMemcpyAsync(&tmp, h->dh, sizeof(kma_heap), cudaMemcpyDeviceToHost, st));
-	if (state)
-		KMA_CUDA(cudaMemcpyAsync(state, h->hh.sb_state, (size_t)h->hh.nsb * 4, cudaMemcpyDeviceToHost, st));
-	if (next)
-		KMA_CUDA(cudaMemcpyAsync(next, h->hh.sb_next, (size_t)h->hh.nsb * 8, cudaMemcpyDeviceToHost, st));
-	if (region_dst && region_len)
-		KMA_CUDA(cudaMemcpyAsync(region_dst, h->hh.sb_base + region_off, region_len,
-				cudaMemcpyDeviceToHost, st));
-	KMA_CUDA(cudaStreamSynchronize(st));
-	if (cls)
-		for (int c = 0; c < 16; c++)
-			cls[c] = tmp.cls[c].v;
-	if (headtail) {
-		headtail[0] = tmp.free_head.v;
-		headtail[1] = tmp.free_tail.v;
+	kma_heap *tmp = (kma_heap *)malloc(sizeof(kma_heap));
+	if (!tmp)
+		return KMA_ENOMEM;
+	const bool ring = h->hh.flags & KMA_HEAP_RING;
+	size_t nw = ring ? h->hh.ring_cap : h->hh.nsb;
+	std::vector<unsigned long long> words;
+	int rc = KMA_OK;
+	if (cudaMemcpyAsync(tmp, h->dh, sizeof(kma_heap), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+		rc = KMA_ECUDA;
+	if (rc == KMA_OK && state &&
+			cudaMemcpyAsync(state, h->hh.sb_state, (size_t)h->hh.nsb * 4, cudaMemcpyDeviceToHost, st) !=
+				cudaSuccess)
+		rc = KMA_ECUDA;
+	if (rc == KMA_OK && freelist) {
+		words.resize(nw);
+		if (cudaMemcpyAsync(words.data(), ring ? h->hh.ring : h->hh.sb_next, nw * 8,
+				    cudaMemcpyDeviceToHost, st) != cudaSuccess)
+			rc = KMA_ECUDA;
 	}
-	return KMA_OK;
+	if (rc == KMA_OK && region_dst && region_len &&
+			cudaMemcpyAsync(region_dst, h->hh.sb_base + region_off, region_len, cudaMemcpyDeviceToHost,
+				st) != cudaSuccess)
+		rc = KMA_ECUDA;
+	if (rc == KMA_OK && cudaStreamSynchronize(st) != cudaSuccess)
+		rc = KMA_ECUDA;
+	if (rc == KMA_OK && cls)
+		for (uint32_t i = 0; i < h->hh.nshards * KMA_MAX_CLASSES; i++)
+			cls[i] = tmp->cls[i].v;
+	if (rc == KMA_OK && freelist) {
+		uint64_t n = 0;
+		if (ring) {
+			uint64_t hd = tmp->free_head.v, tl = tmp->free_tail.v;
+			for (uint64_t p = hd; p < tl && n < h->hh.nsb; p++)
+				freelist[n++] = (uint32_t)words[p % nw];
+			if (tl - hd > h->hh.nsb)
+				n = UINT64_MAX;
+		} else {
+			uint32_t idx = (uint32_t)tmp->free_head.v;
+			while (idx != 0) {
+				if (n >= h->hh.nsb || idx > nw) {
+					n = UINT64_MAX;
+					break;
+				}
+				freelist[n++] = idx - 1;
+				idx = (uint32_t)words[idx - 1];
+			}
+		}
+		if (freelist_len)
+			*freelist_len = n;
+	}
+	free(tmp);
+	return rc;
 }
 
 extern "C" int kma_gather_bitmaps(kma_heap_t h, void *stream, uint32_t *dst, uint32_t words)
@@ -424,8 +508,11 @@ extern "C" int kma_debug_set_class_word(kma_heap_t h, uint32_t cls, uint32_t val
 	if (!h || cls >= h->hh.nclasses)
 		return KMA_EINVAL;
 	kma_device_guard g(h->device);
-	static_assert(sizeof(uint32_t) == 4, "u32");
-	KMA_CUDA(cudaMemcpyAsync(&h->dh->cls[cls].v, &value, 4, cudaMemcpyHostToDevice, kma_stream(stream)));
-	KMA_CUDA(cudaStreamSynchronize(kma_stream(stream)));
+	cudaStream_t st = kma_stream(stream);
+	/* every shard's word of the class, so any calling SM sees it */
+	for (uint32_t s = 0; s < h->hh.nshards; s++)
+		KMA_CUDA(cudaMemcpyAsync(&h->dh->cls[s * KMA_MAX_CLASSES + cls].v, &value, 4,
+					 cudaMemcpyHostToDevice, st));
+	KMA_CUDA(cudaStreamSynchronize(st));
 	return KMA_OK;
 }

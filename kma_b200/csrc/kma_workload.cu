@@ -285,30 +285,67 @@ __device__ __forceinline__ void flush_counters(const wl_dev &w, uint32_t mask, u
 	}
 }
 
+/* Persistent, round-major: the grid holds only as many threads as stay
+ * resident; when there are more items than threads each thread walks the
+ * items g = tid, tid+T, ... inside every round, so every item finishes
+ * round r before any starts round r+1 -- as if all of them ran at once.
+ * (Launching one thread per item instead lets early waves finish all
+ * their rounds and pin their last live blocks while later waves start,
+ * which fragments the heap far beyond what concurrent items do.) */
 template <int MODE>
 __global__ void __launch_bounds__(256) k_wl_rounds(kma_heap *h, wl_dev w, uint32_t nrounds, int drain)
 {
 	const uint32_t mask = 0xffffffffu;
 	const uint32_t lane = threadIdx.x & 31;
-	uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	bool act = g < w.items;
-	wl_item it;
-	it.rng = act ? w.rng[g] : 0;
-	it.hash = act ? w.hash[g] : 0;
-	it.nlive = act ? w.nlive[g] : 0;
+	const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+	const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	wl_counters ct = {0, 0, 0, 0, 0, 0};
-	for (uint32_t r = 0; r < nrounds; r++) {
-		if (w.program == KMA_WL_C1)
-			c1_round<MODE>(h, mask, lane, act, g, it, ct);
-		else
-			c2_round<MODE>(h, w, mask, lane, act, g, it, ct);
-	}
-	if (drain && w.program == KMA_WL_C2)
-		c2_drain<MODE>(h, w, mask, lane, act, g, it, ct);
-	if (act) {
-		w.rng[g] = it.rng;
-		w.hash[g] = it.hash;
-		w.nlive[g] = it.nlive;
+	const bool c2 = w.program == KMA_WL_C2;
+	if (w.items <= T) {
+		/* one item per thread: its state stays in registers */
+		uint64_t g = tid;
+		bool act = g < w.items;
+		wl_item it;
+		it.rng = act ? w.rng[g] : 0;
+		it.hash = act ? w.hash[g] : 0;
+		it.nlive = act ? w.nlive[g] : 0;
+		for (uint32_t r = 0; r < nrounds; r++) {
+			if (c2)
+				c2_round<MODE>(h, w, mask, lane, act, g, it, ct);
+			else
+				c1_round<MODE>(h, mask, lane, act, g, it, ct);
+		}
+		if (drain && c2)
+			c2_drain<MODE>(h, w, mask, lane, act, g, it, ct);
+		if (act) {
+			w.rng[g] = it.rng;
+			w.hash[g] = it.hash;
+			w.nlive[g] = it.nlive;
+		}
+	} else {
+		for (uint32_t r = 0; r <= nrounds; r++) {
+			if (r == nrounds && !(drain && c2))
+				break;
+			for (uint64_t base = 0; base < w.items; base += T) {
+				uint64_t g = base + tid;
+				bool act = g < w.items;
+				wl_item it;
+				it.rng = act ? w.rng[g] : 0;
+				it.hash = act ? w.hash[g] : 0;
+				it.nlive = act ? w.nlive[g] : 0;
+				if (r == nrounds)
+					c2_drain<MODE>(h, w, mask, lane, act, g, it, ct);
+				else if (c2)
+					c2_round<MODE>(h, w, mask, lane, act, g, it, ct);
+				else
+					c1_round<MODE>(h, mask, lane, act, g, it, ct);
+				if (act) {
+					w.rng[g] = it.rng;
+					w.hash[g] = it.hash;
+					w.nlive[g] = it.nlive;
+				}
+			}
+		}
 	}
 	flush_counters(w, mask, lane, ct);
 }
@@ -507,6 +544,15 @@ static int wl_launch(kma_wl_t w, uint32_t nrounds, int mode, uint32_t bd, int dr
 	kma_device_guard g(w->heap->device);
 	cudaStream_t st = kma_stream(stream);
 	uint32_t nb = wl_blocks(w->d.items, bd);
+	/* persistent grid: no more blocks than stay resident on all SMs */
+	int per_sm = 0, sms = 0;
+	const void *fn = mode == KMA_MODE_WARP ? (const void *)k_wl_rounds<KMA_MODE_WARP>
+					       : (const void *)k_wl_rounds<KMA_MODE_PLAIN>;
+	KMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)bd, 0));
+	KMA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, w->heap->device));
+	uint64_t resident = (uint64_t)(per_sm > 0 ? per_sm : 1) * (uint64_t)(sms > 0 ? sms : 1);
+	if (nb > resident)
+		nb = (uint32_t)resident;
 	if (mode == KMA_MODE_WARP)
 		k_wl_rounds<KMA_MODE_WARP><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain);
 	else

@@ -49,9 +49,10 @@ class Heap:
     """
 
     def __init__(self, sblocks: int, sb_size_log2: int = 12, spin_limit: int = 0,
-                 device: int = -1, stream=None):
+                 device: int = -1, stream=None, shards: int = 0, compat: bool = False):
         L = lib()
-        cfg = KmaConfig(sblocks, sb_size_log2, spin_limit, device)
+        cfg = KmaConfig(sblocks, sb_size_log2, spin_limit, device, shards,
+                        _lib.KMA_CFG_COMPAT if compat else 0)
         h = c_void_p()
         check(L.kma_create_ex(byref(cfg), _stream_ptr(stream), byref(h)), "kma_create")
         self._h = h
@@ -67,6 +68,8 @@ class Heap:
         self.device_bytes = int(inf.device_bytes)
         self.cls_size = [int(inf.cls_size[i]) for i in range(self.nclasses)]
         self.cls_slots = [int(inf.cls_slots[i]) for i in range(self.nclasses)]
+        self.nshards = int(inf.nshards)
+        self.compat = bool(inf.flags & _lib.KMA_CFG_COMPAT)
 
     # -- lifetime ---------------------------------------------------------
     @property
@@ -128,20 +131,21 @@ class Heap:
         """Copy the heap's metadata (and optionally its superblock region) to
         host numpy arrays; see ``kma_b200.inspect``."""
         from .inspect import HeapImage
-        cls = np.zeros(16, np.uint32)
-        ht = np.zeros(2, np.uint64)
+        cls = np.zeros(self.nshards * 16, np.uint32)
         state = np.zeros(self.sblocks, np.uint32)
-        nxt = np.zeros(self.sblocks, np.uint64)
+        fl = np.zeros(self.sblocks, np.uint32)
+        fl_len = np.zeros(1, np.uint64)
         reg = np.zeros(self.region_bytes if region else 0, np.uint8)
         check(lib().kma_snapshot(self.handle, _stream_ptr(stream), cls.ctypes.data,
-                                 ht.ctypes.data, state.ctypes.data, nxt.ctypes.data, 0,
+                                 state.ctypes.data, fl.ctypes.data, fl_len.ctypes.data, 0,
                                  self.region_bytes if region else 0,
                                  reg.ctypes.data if region else None), "kma_snapshot")
+        n = int(fl_len[0])
+        freelist = None if n == 2**64 - 1 else fl[:n].astype(np.int64)
         return HeapImage(sb_size_log2=self.sb_size_log2, sblocks=self.sblocks, pages=self.pages,
                          nclasses=self.nclasses, cls_size=list(self.cls_size),
-                         cls_slots=list(self.cls_slots), cls_raw=cls, head=int(ht[0]),
-                         tail=int(ht[1]), state=state, next=nxt,
-                         region=reg if region else None)
+                         cls_slots=list(self.cls_slots), cls_raw=cls.reshape(self.nshards, 16),
+                         state=state, freelist=freelist, region=reg if region else None)
 
     # -- serial replay ------------------------------------------------------
     def replay(self, ops: np.ndarray, mode: int = _lib.MODE_PLAIN) -> np.ndarray:

@@ -3,9 +3,13 @@ the reference, and check heap invariants.
 
 Canonical form (implementation-neutral, what serial replay compares):
   cls[c]       superblock attached to class c, -1 empty, -2 POISON
+               (a sharded heap attaches at most one superblock per class
+               under serial execution; several shards holding one is
+               reported as -3)
   sb_size[s]   block size of superblock s (0 if never used)
   sb_slots[s]  slots, sb_free[s] free count (kma.cl:180 packs slots<<16|free)
-  freelist     superblock indices from the head (the dummy) to the tail
+  freelist     superblock indices in FIFO order, the next one handed out
+               (the reference's dummy, clIndexedQueue.cl:282-289) first
   region       superblock bytes with each superblock's first 12 bytes
                masked (header fields live elsewhere here), i.e. the
                bitmaps and the word-0 residue malloc/free leave in blocks
@@ -29,11 +33,9 @@ class HeapImage:
     nclasses: int
     cls_size: list
     cls_slots: list
-    cls_raw: np.ndarray
-    head: int
-    tail: int
-    state: np.ndarray
-    next: np.ndarray
+    cls_raw: np.ndarray          # (nshards, 16) raw class-table words
+    state: np.ndarray            # (sblocks,) class<<28 | slots<<14 | free
+    freelist: np.ndarray | None  # FIFO order; None if the list has a cycle
     region: np.ndarray | None = None
 
 
@@ -49,27 +51,25 @@ class Canonical:
 
 
 def decode(img: HeapImage) -> Canonical:
-    raw = img.cls_raw[: img.nclasses].astype(np.int64)
-    cls = np.where(raw == 0, -1, np.where(raw == 1, -2, raw - 2)).astype(np.int64)
+    raw = np.asarray(img.cls_raw, np.int64).reshape(-1, 16)[:, : img.nclasses]
+    cls = np.full(img.nclasses, -1, np.int64)
+    for c in range(img.nclasses):
+        col = raw[:, c]
+        nz = col[col != 0]
+        if len(nz) > 1:
+            cls[c] = -3
+        elif len(nz) == 1:
+            cls[c] = -2 if nz[0] == 1 else nz[0] - 2
     st = img.state.astype(np.uint64)
     cl = (st >> 28).astype(np.int64)
     slots = ((st >> 14) & FREE_MASK).astype(np.uint32)
     free = (st & FREE_MASK).astype(np.uint32)
     sizes = np.asarray(img.cls_size + [0] * (16 - len(img.cls_size)), np.uint32)
     size = np.where(st == 0, 0, sizes[np.clip(cl, 0, 15)]).astype(np.uint32)
-    fl = []
-    idx = int(img.head) & 0xFFFFFFFF
-    limit = img.sblocks + 1
-    nxt = img.next
-    while idx != 0:
-        if len(fl) > limit:
-            fl = None
-            break
-        fl.append(idx - 1)
-        idx = int(nxt[idx - 1]) & 0xFFFFFFFF
     canon = Canonical(cls=cls, sb_size=size, sb_slots=slots, sb_free=free,
-                      freelist=np.asarray(fl if fl is not None else [-1], np.int64))
-    if fl is None:
+                      freelist=np.asarray(img.freelist if img.freelist is not None else [-1],
+                                          np.int64))
+    if img.freelist is None:
         canon.notes.append("free list does not terminate (cycle)")
     if img.region is not None:
         canon.region = mask_headers(img.region, img.sb_size_log2)
@@ -92,11 +92,12 @@ def bitmap_words(region: np.ndarray, sb_size_log2: int, s: int, words: int) -> n
 
 def check_canonical_empty(img: HeapImage, bitmaps: np.ndarray | None = None) -> list[str]:
     """The state every heap returns to once all blocks are freed: no class
-    attached, every page on the free list exactly once, every bitmap of a
-    used superblock clear (from img.region, or bitmaps[s, k] when given)."""
+    attached in any shard, every page on the free list exactly once, every
+    bitmap of a used superblock clear (from img.region, or bitmaps[s, k]
+    when given)."""
     c = decode(img)
     bad = []
-    if np.any(c.cls != -1):
+    if np.any(np.asarray(img.cls_raw) != 0):
         bad.append(f"class table not empty: {c.cls.tolist()}")
     fl = c.freelist
     if c.notes:

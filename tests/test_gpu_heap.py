@@ -27,6 +27,10 @@ REPLAYS = sorted(glob.glob(os.path.join(GOLD, "replay_*.npz")))
 WORKLOADS = json.load(open(os.path.join(GOLD, "workloads.json")))
 MODES = [MODE_PLAIN, MODE_WARP]
 MODE_IDS = ["plain", "warp"]
+# heap structures: the reference's (one class table, tagged-CAS MS queue),
+# the default (ticket-ring free list, shards by size), and 8 shards forced
+HEAPS = [dict(compat=True), dict(), dict(shards=8)]
+HEAP_IDS = ["compat", "default", "shards8"]
 
 
 def digest(a):
@@ -49,12 +53,13 @@ def test_create_matches_reference_initial_state():
         assert h.error_flags() == 0
 
 
+@pytest.mark.parametrize("heap", HEAPS, ids=HEAP_IDS)
 @pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("path", REPLAYS, ids=os.path.basename)
-def test_replay_matches_golden(path, mode):
+def test_replay_matches_golden(path, mode, heap):
     g = np.load(path)
     log2 = int(os.path.basename(path).split("_")[1])
-    with Heap(int(g["sblocks"]), log2) as h:
+    with Heap(int(g["sblocks"]), log2, **heap) as h:
         out = h.replay(g["ops"], mode)
         assert np.array_equal(out, g["out"]), np.nonzero(out != g["out"])[0][:5]
         canon = ins.decode(h.snapshot(region=True))
@@ -66,9 +71,10 @@ def test_replay_matches_golden(path, mode):
 @pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("log2,sblocks,seed", [(12, 33, 21), (12, 300, 22), (14, 11, 23),
                                                (16, 7, 24), (12, 2, 25), (12, 3, 26)])
-def test_replay_matches_port_live(log2, sblocks, seed, mode):
+@pytest.mark.parametrize("heap", HEAPS[:2], ids=HEAP_IDS[:2])
+def test_replay_matches_port_live(log2, sblocks, seed, mode, heap):
     ops = drain_stream(make_stream(seed, 2500, log2))
-    with Heap(sblocks, log2) as h, oracle.Port(sblocks, log2) as p:
+    with Heap(sblocks, log2, **heap) as h, oracle.Port(sblocks, log2) as p:
         want = p.replay(ops)
         got = h.replay(ops, mode)
         assert np.array_equal(got, want)
@@ -77,7 +83,8 @@ def test_replay_matches_port_live(log2, sblocks, seed, mode):
         assert np.array_equal(canon.region, p.region())
 
 
-def test_replay_beyond_reference_index_limit():
+@pytest.mark.parametrize("heap", HEAPS[:2], ids=HEAP_IDS[:2])
+def test_replay_beyond_reference_index_limit(heap):
     # 70 000 superblocks: past the reference's 16-bit queue index; the port
     # (widened index) is the oracle here
     sblocks = 70000
@@ -85,7 +92,7 @@ def test_replay_beyond_reference_index_limit():
     ops = np.zeros((2 * n, 2), np.int64)
     ops[:n, 0], ops[:n, 1] = 0, 2000
     ops[n:, 0], ops[n:, 1] = 1, np.arange(n)
-    with Heap(sblocks, 12) as h, oracle.Port(sblocks, 12) as p:
+    with Heap(sblocks, 12, **heap) as h, oracle.Port(sblocks, 12) as p:
         assert np.array_equal(h.replay(ops), p.replay(ops))
         assert_canon(ins.decode(h.snapshot()), p.decode())
 
@@ -103,11 +110,13 @@ def test_reset_restores_initial_state():
             assert np.array_equal(h.replay(ops), p.replay(ops))
 
 
+@pytest.mark.parametrize("heap", HEAPS[:2], ids=HEAP_IDS[:2])
 @pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
 @pytest.mark.parametrize("name", sorted(WORKLOADS))
-def test_serial_workload_matches_golden(name, mode):
+def test_serial_workload_matches_golden(name, mode, heap):
     w = WORKLOADS[name]
-    with Heap(w["sblocks"], w["sb_size_log2"]) as h, Workload(h, w["program"], w["items"]) as wl:
+    with Heap(w["sblocks"], w["sb_size_log2"], **heap) as h, \
+            Workload(h, w["program"], w["items"]) as wl:
         wl.begin(w["seed"])
         wl.serial(w["rounds"], bool(w["round_major"]), mode)
         st = wl.stats()
@@ -118,10 +127,11 @@ def test_serial_workload_matches_golden(name, mode):
         assert h.error_flags() == 0
 
 
+@pytest.mark.parametrize("heap", HEAPS, ids=HEAP_IDS)
 @pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
-def test_c1_concurrent(mode):
+def test_c1_concurrent(mode, heap):
     # config 1: 16 MiB heap of 4 KiB superblocks, 4 x 64 items, 16 rounds
-    with Heap(4096, 12) as h, Workload(h, WL_C1, 256) as wl:
+    with Heap(4096, 12, **heap) as h, Workload(h, WL_C1, 256) as wl:
         wl.begin(0xC1)
         wl.rounds(16, mode, block_dim=64)
         st = wl.stats()
@@ -132,15 +142,19 @@ def test_c1_concurrent(mode):
         assert h.error_flags() == 0
 
 
-@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
-def test_c2_full_size_invariants(mode):
+@pytest.mark.parametrize("mode,heap", [(MODE_PLAIN, dict(compat=True)), (MODE_PLAIN, dict()),
+                                       (MODE_WARP, dict(compat=True)), (MODE_WARP, dict())],
+                         ids=["plain-compat", "plain-default", "warp-compat", "warp-default"])
+def test_c2_full_size_invariants(mode, heap):
     # config 2: 1 GiB heap of 16 KiB superblocks, 148 x 2048 items, 64 rounds
     items = 148 * 2048
-    with Heap(65536, 14) as h, Workload(h, WL_C2, items) as wl:
+    with Heap(65536, 14, **heap) as h, Workload(h, WL_C2, items) as wl:
         wl.begin(0xC2)
         wl.rounds(64, mode)
         st = wl.stats()
         assert st["bad_tags"] == 0 and st["mallocs"] == items * 64
+        # round-major execution keeps this heap far from exhaustion
+        assert st["nulls"] <= st["mallocs"] // 100
         nlive, off, size = wl.live()
         sel = np.arange(off.shape[0])[:, None] < nlive[None, :]
         live_off, live_size = off[sel], size[sel]
@@ -159,8 +173,8 @@ def test_c2_full_size_invariants(mode):
 
 def test_double_free_is_refused_not_corrupting():
     ops = np.array([[0, 64], [0, 64], [1, 0], [1, 0], [1, 1]], np.int64)
-    for mode in MODES:
-        with Heap(16, 12) as h:
+    for mode, heap in zip(MODES * 2, [HEAPS[0]] * 2 + [HEAPS[1]] * 2):
+        with Heap(16, 12, **heap) as h:
             h.replay(ops, mode)
             assert h.error_flags(clear=True) & kma_b200.KMA_FLAG_BADFREE
             img = h.snapshot()
@@ -170,8 +184,8 @@ def test_double_free_is_refused_not_corrupting():
 def test_bounded_wait_times_out_without_fault():
     # a class word stuck at POISON (nothing will clear it): every request
     # of that class gives up after spin_limit iterations and returns NULL
-    for mode in MODES:
-        with Heap(32, 12, spin_limit=2000) as h:
+    for mode, heap in zip(MODES * 2, [HEAPS[0]] * 2 + [HEAPS[2]] * 2):
+        with Heap(32, 12, spin_limit=2000, **heap) as h:
             h.debug_set_class_word(2, 1)
             out = h.replay(np.array([[0, 16], [0, 8]], np.int64), mode)
             assert out[0] == -1  # class 2 (16 B): timed out

@@ -15,16 +15,11 @@ def image_from_port(p, sblocks, log2, ops, out):
         if d["sb_slots"][s]:
             c = sizes.index(int(d["sb_size"][s]))
             st[s] = (c << 28) | (int(d["sb_slots"][s]) << 14) | int(d["sb_free"][s])
-    cls = np.zeros(16, np.uint32)
+    cls = np.zeros((1, 16), np.uint32)
     for c, v in enumerate(d["cls"]):
-        cls[c] = 0 if v == -1 else 1 if v == -2 else v + 2
-    nxt = np.zeros(sblocks, np.uint64)
-    fl = d["freelist"]
-    for a, b in zip(fl[:-1], fl[1:]):
-        nxt[a] = b + 1
+        cls[0, c] = 0 if v == -1 else 1 if v == -2 else v + 2
     img = ins.HeapImage(log2, sblocks, sblocks - 1, log2 - 1, sizes,
-                        oracle.port_tables(log2)[1], cls, int(fl[0]) + 1, int(fl[-1]) + 1,
-                        st, nxt, p.region())
+                        oracle.port_tables(log2)[1], cls, st, d["freelist"].copy(), p.region())
     return img, d
 
 
