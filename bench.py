@@ -342,7 +342,7 @@ def run_ours(args) -> int:
                        "parallelism": f"replicas x{world}",
                        "plain_mops": round(plain, 3) if plain else None,
                        "plain_default_heap_mops": round(plain_default, 3) if plain_default else None,
-                       "shards": heap.nshards,
+                       "class_shards": heap.cls_shards,
                        "warp_over_plain": round(value / world / plain, 2) if plain else None},
             "roofline": {"bound": "hbm", "kernel": "k_wl_rounds<warp>",
                          "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",

@@ -54,8 +54,10 @@ typedef struct kma_config {
 	uint32_t sb_size_log2; /* 12..16: 4 KiB (the reference's KMA_SB_SIZE, kma.h:27) .. 64 KiB */
 	uint32_t spin_limit;   /* bound on every device spin; 0 = default (1<<22) */
 	int32_t device;        /* CUDA ordinal; -1 = current device */
-	uint32_t shards;       /* class-table shards (1..64), a thread uses smid % shards;
-				* 0 = default: min(64, max(1, (sblocks-1)/1024)); 1 with COMPAT */
+	uint32_t shards;       /* most class-table shards per class (1..512); a warp uses
+				* shard (global warp id) % shards(class).  Each class gets
+				* (sblocks-1)/32/slots(class) shards, clamped to [1, shards];
+				* 0 = 512.  COMPAT forces 1 (the reference's single table) */
 	uint32_t flags;        /* KMA_CFG_* */
 } kma_config;
 
@@ -66,7 +68,8 @@ typedef struct kma_info {
 	uint32_t max_request;    /* largest request served: SB - 16 (kma.cl:126) */
 	uint32_t cls_size[16];   /* block size per class (kma.cl:55-90) */
 	uint32_t cls_slots[16];  /* slots per superblock per class (kma.cl:95-113) */
-	uint32_t nshards;
+	uint32_t cls_shards[16]; /* class-table shards per class */
+	uint32_t cls_lines;      /* class-table words in all: sum of cls_shards */
 	uint32_t flags;          /* KMA_CFG_* in effect */
 } kma_info;
 
@@ -104,8 +107,9 @@ const char *kma_version(void);
 
 /* ---- heap image for checkers ------------------------------------------ */
 /* Copies to host (any NULL destination is skipped), synchronising stream:
- *   cls[nshards*16]  raw class-table words, shard-major (0 empty, 1 POISON,
- *                    s+2 superblock s)
+ *   cls[cls_lines]   raw class-table words, class-major: class c's shards
+ *                    are words [sum of cls_shards[<c]] .. + cls_shards[c]
+ *                    (0 empty, 1 POISON, s+2 superblock s)
  *   state[sblocks]   class<<28 | slots<<14 | free
  *   freelist[sblocks], *freelist_len: the superblock free list in FIFO
  *                    order, head (the next one handed out) first; length

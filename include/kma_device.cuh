@@ -12,7 +12,7 @@
  * and the PMA bump heap are in kma_structs.cuh.
  *
  * Heap layout in HBM (one cudaMalloc per heap, owned by kma_create):
- *   [kma_heap header | sb_state[nsb] u32 | sb_home[nsb] u8 |
+ *   [kma_heap header | sb_state[nsb] u32 | sb_home[nsb] u16 |
  *    free-list words | superblocks]
  *   Superblock s lives at sb_base + s*SB: bytes [0,12) are reserved so that
  *   every block offset equals the reference's (its in-band 12-byte header,
@@ -23,11 +23,17 @@
  *   slots<<16 | free, kma.cl:180; the class field makes a stale reservation
  *   detectable) and sb_home[s] = the shard whose class table holds s.
  *
- * Class table (kma.h:84): word cls[shard][c] is 0 (empty), 1 (POISON,
- * refill in progress) or s+2 (superblock s is the current one for class c
- * in that shard).  Every hot word sits on its own 128-byte line.  A thread
- * uses shard smid % nshards; a heap with one shard is the reference's
- * single table.
+ * Class table (kma.h:84): each class c has cls_nsh[c] words ("shards"),
+ * each 0 (empty), 1 (POISON, refill in progress) or s+2 (superblock s is
+ * that shard's current superblock for class c), every one on its own
+ * 128-byte line.  A warp uses shard (global warp id) % cls_nsh[c], so one
+ * thread of warp 0 -- a serial replay -- always uses shard 0; a heap with
+ * one shard per class is the reference's single table.  Only a
+ * superblock's current slots are contended, and a class with few slots per
+ * superblock refills that many times more often, so kma_create gives each
+ * class shards in inverse proportion to its slots (the few-slot classes get
+ * the most parallel refill streams) within a budget of pinned current
+ * superblocks proportional to the heap.
  *
  * Superblock free list, FIFO with the reference's order and its rule that
  * one superblock always stays behind as the queue's dummy
@@ -55,7 +61,8 @@
 #include <stddef.h>
 
 #define KMA_MAX_CLASSES 16
-#define KMA_MAX_SHARDS 64
+#define KMA_MAX_SHARDS 512     /* per class */
+#define KMA_MAX_CLS_LINES 8192 /* sum over classes */
 #define KMA_SB_HDR 12u
 #define KMA_POISON 1u
 #define KMA_CLS_BASE 2u
@@ -84,7 +91,7 @@ struct __align__(128) kma_heap {
 	/* geometry: written by kma_create, read-only afterwards */
 	unsigned char *sb_base;
 	uint32_t *sb_state;
-	uint8_t *sb_home;
+	uint16_t *sb_home;
 	unsigned long long *sb_next; /* MS-queue links [nsb] (no KMA_HEAP_RING) */
 	unsigned long long *ring;    /* ring slots [ring_cap] (KMA_HEAP_RING) */
 	unsigned long long region_bytes; /* nsb << sb_log2 */
@@ -96,8 +103,10 @@ struct __align__(128) kma_heap {
 	uint32_t max_request;/* SB - 16 (kma.cl:126) */
 	uint32_t spin_limit;
 	uint32_t flags;
-	uint32_t nshards;
+	uint32_t cls_lines;  /* sum of cls_nsh[] */
 	uint32_t ring_cap;
+	uint32_t cls_nsh[KMA_MAX_CLASSES];   /* shards per class */
+	uint32_t cls_base[KMA_MAX_CLASSES];  /* first line of the class in cls[] */
 	uint32_t cls_size[KMA_MAX_CLASSES];  /* kma.cl:55-90 */
 	uint32_t cls_slots[KMA_MAX_CLASSES]; /* kma.cl:95-113 */
 	uint32_t cls_magic[KMA_MAX_CLASSES]; /* floor(2^32/size)+1: exact x/size for x < 2^16 */
@@ -107,7 +116,7 @@ struct __align__(128) kma_heap {
 	kma_line64 free_tail; /* MS-queue tail, or ring tail ticket */
 	kma_line32 ring_avail;
 	kma_line32 err;
-	kma_line32 cls[KMA_MAX_SHARDS * KMA_MAX_CLASSES];
+	kma_line32 cls[KMA_MAX_CLS_LINES];
 };
 
 /* ------------------------------------------------------------------ */
@@ -257,14 +266,22 @@ __device__ __forceinline__ uint32_t *bitmap_word(const kma_heap *h, unsigned cha
 {
 	return reinterpret_cast<uint32_t *>(sb + h->sb_size) - 1 - k;
 }
-__device__ __forceinline__ uint32_t my_shard(const kma_heap *h)
+/* linear id of the calling warp in the grid (stable for its lifetime) */
+__device__ __forceinline__ unsigned long long global_warp()
 {
-	uint32_t n = h->nshards;
-	return n > 1 ? sm_id() % n : 0u;
+	unsigned long long blk = ((unsigned long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+	uint32_t tpb = blockDim.x * blockDim.y * blockDim.z;
+	uint32_t t = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+	return blk * ((tpb + 31) / 32) + t / 32;
 }
-__device__ __forceinline__ uint32_t *cls_word(kma_heap *h, uint32_t shard, uint32_t c)
+__device__ __forceinline__ uint32_t my_shard(const kma_heap *h, uint32_t c)
 {
-	return &h->cls[shard * KMA_MAX_CLASSES + c].v;
+	uint32_t n = h->cls_nsh[c];
+	return n > 1 ? (uint32_t)(global_warp() % n) : 0u;
+}
+__device__ __forceinline__ uint32_t *cls_word(kma_heap *h, uint32_t c, uint32_t shard)
+{
+	return &h->cls[h->cls_base[c] + shard].v;
 }
 
 } /* namespace kma_detail */
@@ -439,7 +456,7 @@ __device__ __forceinline__ void sb_format(kma_heap *h, uint32_t s, uint32_t c, u
 		}
 		*bitmap_word(h, sb, k) = v;
 	}
-	h->sb_home[s] = (uint8_t)shard;
+	h->sb_home[s] = (uint16_t)shard;
 	fence_acqrel();
 	st_release(&h->sb_state[s], st_make(c, slots, fr));
 }
@@ -504,8 +521,8 @@ __device__ inline void *kma_malloc(kma_heap *h, size_t size)
 	int c = kma_class_of(h, size);
 	if (c < 0)
 		return NULL;
-	uint32_t shard = my_shard(h);
-	uint32_t *clsw = cls_word(h, shard, (uint32_t)c);
+	uint32_t shard = my_shard(h, (uint32_t)c);
+	uint32_t *clsw = cls_word(h, (uint32_t)c, shard);
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
 		/* kma.cl:163: CAS 0 -> POISON doubles as the read of the slot */
@@ -571,7 +588,7 @@ __device__ __forceinline__ bool block_locate(const kma_heap *h, const void *p, u
 __device__ __forceinline__ void sb_recycle(kma_heap *h, uint32_t s, uint32_t c)
 {
 	uint32_t home = h->sb_home[s];
-	cas_acqrel(cls_word(h, home, c), s + KMA_CLS_BASE, 0);
+	cas_acqrel(cls_word(h, c, home), s + KMA_CLS_BASE, 0);
 	sb_enqueue(h, s);
 }
 } /* namespace kma_detail */
@@ -643,7 +660,7 @@ struct warp_resv {
 __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t want, warp_resv &r)
 {
 	uint32_t slots = h->cls_slots[c];
-	uint32_t shard = my_shard(h);
+	uint32_t shard = my_shard(h, c);
 	if (want >= slots && slots > 1) {
 		/* the group fills a whole superblock: take a fresh one privately
 		 * (it would be detached at once anyway) */
@@ -660,7 +677,7 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		r.pre = true;
 		return 1;
 	}
-	uint32_t *clsw = cls_word(h, shard, c);
+	uint32_t *clsw = cls_word(h, c, shard);
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
 		uint32_t cur = ld_acquire(clsw);

@@ -52,7 +52,7 @@ class KmaInfo(Structure):
                 ("sblocks", c_uint32), ("pages", c_uint32), ("sb_size_log2", c_uint32),
                 ("nclasses", c_uint32), ("max_request", c_uint32),
                 ("cls_size", c_uint32 * 16), ("cls_slots", c_uint32 * 16),
-                ("nshards", c_uint32), ("flags", c_uint32)]
+                ("cls_shards", c_uint32 * 16), ("cls_lines", c_uint32), ("flags", c_uint32)]
 
 
 class KmaWlStats(Structure):

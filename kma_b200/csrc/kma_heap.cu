@@ -138,7 +138,7 @@ __global__ void kma_k_reset(kma_heap *h, uint32_t nsb, uint32_t nfree)
 		else
 			w[i] = (s + 1 < nfree) ? tw_make(0, s + 2) : 0ull;
 	}
-	for (uint64_t i = tid; i < (uint64_t)KMA_MAX_SHARDS * KMA_MAX_CLASSES; i += stride)
+	for (uint64_t i = tid; i < h->cls_lines; i += stride)
 		h->cls[i].v = 0;
 	if (tid == 0) {
 		if (ring) {
@@ -241,20 +241,30 @@ extern "C" int kma_create_ex(const kma_config *cfg, void *stream, kma_heap_t *ou
 	 * header, i.e. sblocks - 1 superblocks enter the free list */
 	k->hh.pages = (uint32_t)nsb - 1;
 	const bool compat = cfg->flags & KMA_CFG_COMPAT;
-	uint32_t shards = cfg->shards;
-	if (compat)
-		shards = 1;
-	else if (shards == 0) {
-		shards = k->hh.pages / 1024;
-		shards = shards < 1 ? 1 : shards > KMA_MAX_SHARDS ? KMA_MAX_SHARDS : shards;
+	/* shards per class: a budget of pinned current superblocks of pages/32
+	 * (about 3% of the heap if every shard of every class held one),
+	 * divided among the classes in inverse proportion to their slots, at
+	 * most cfg->shards (default KMA_MAX_SHARDS) per class */
+	uint32_t cap = compat ? 1u : (cfg->shards ? cfg->shards : KMA_MAX_SHARDS);
+	uint32_t budget = k->hh.pages / 32;
+	uint32_t lines = 0;
+	for (uint32_t c = 0; c < KMA_MAX_CLASSES; c++) {
+		uint32_t n = 0;
+		if (c < k->hh.nclasses) {
+			n = budget / k->hh.cls_slots[c];
+			n = n < 1 ? 1 : n > cap ? cap : n;
+		}
+		k->hh.cls_nsh[c] = n;
+		k->hh.cls_base[c] = lines;
+		lines += n;
 	}
-	k->hh.nshards = shards;
+	k->hh.cls_lines = lines;
 	k->hh.flags = compat ? 0u : KMA_HEAP_RING;
 	k->hh.ring_cap = kma_nfree(k->hh);
 
 	size_t hdr = kma_align_up(sizeof(kma_heap), 4096);
 	size_t st_bytes = kma_align_up(nsb * 4, 4096);
-	size_t home_bytes = kma_align_up(nsb, 4096);
+	size_t home_bytes = kma_align_up(nsb * 2, 4096);
 	size_t fl_bytes = kma_align_up((compat ? nsb : k->hh.ring_cap) * 8, 4096);
 	size_t region = (size_t)nsb << cfg->sb_size_log2;
 	size_t total = hdr + st_bytes + home_bytes + fl_bytes + region;
@@ -269,7 +279,7 @@ extern "C" int kma_create_ex(const kma_config *cfg, void *stream, kma_heap_t *ou
 	size_t o = hdr;
 	k->hh.sb_state = (uint32_t *)(base + o);
 	o += st_bytes;
-	k->hh.sb_home = (uint8_t *)(base + o);
+	k->hh.sb_home = (uint16_t *)(base + o);
 	o += home_bytes;
 	if (compat)
 		k->hh.sb_next = (unsigned long long *)(base + o);
@@ -352,7 +362,9 @@ extern "C" int kma_get_info(kma_heap_t h, kma_info *o)
 		o->cls_size[c] = h->hh.cls_size[c];
 		o->cls_slots[c] = h->hh.cls_slots[c];
 	}
-	o->nshards = h->hh.nshards;
+	for (int c = 0; c < 16; c++)
+		o->cls_shards[c] = h->hh.cls_nsh[c];
+	o->cls_lines = h->hh.cls_lines;
 	o->flags = (h->hh.flags & KMA_HEAP_RING) ? 0u : KMA_CFG_COMPAT;
 	return KMA_OK;
 }
@@ -422,7 +434,7 @@ extern "C" int kma_snapshot(kma_heap_t h, void *stream, uint32_t *cls, uint32_t 
 	if (rc == KMA_OK && cudaStreamSynchronize(st) != cudaSuccess)
 		rc = KMA_ECUDA;
 	if (rc == KMA_OK && cls)
-		for (uint32_t i = 0; i < h->hh.nshards * KMA_MAX_CLASSES; i++)
+		for (uint32_t i = 0; i < h->hh.cls_lines; i++)
 			cls[i] = tmp->cls[i].v;
 	if (rc == KMA_OK && freelist) {
 		uint64_t n = 0;
@@ -510,8 +522,8 @@ extern "C" int kma_debug_set_class_word(kma_heap_t h, uint32_t cls, uint32_t val
 	kma_device_guard g(h->device);
 	cudaStream_t st = kma_stream(stream);
 	/* every shard's word of the class, so any calling SM sees it */
-	for (uint32_t s = 0; s < h->hh.nshards; s++)
-		KMA_CUDA(cudaMemcpyAsync(&h->dh->cls[s * KMA_MAX_CLASSES + cls].v, &value, 4,
+	for (uint32_t s = 0; s < h->hh.cls_nsh[cls]; s++)
+		KMA_CUDA(cudaMemcpyAsync(&h->dh->cls[h->hh.cls_base[cls] + s].v, &value, 4,
 					 cudaMemcpyHostToDevice, st));
 	KMA_CUDA(cudaStreamSynchronize(st));
 	return KMA_OK;

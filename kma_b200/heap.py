@@ -68,7 +68,8 @@ class Heap:
         self.device_bytes = int(inf.device_bytes)
         self.cls_size = [int(inf.cls_size[i]) for i in range(self.nclasses)]
         self.cls_slots = [int(inf.cls_slots[i]) for i in range(self.nclasses)]
-        self.nshards = int(inf.nshards)
+        self.cls_shards = [int(inf.cls_shards[i]) for i in range(self.nclasses)]
+        self.cls_lines = int(inf.cls_lines)
         self.compat = bool(inf.flags & _lib.KMA_CFG_COMPAT)
 
     # -- lifetime ---------------------------------------------------------
@@ -131,7 +132,7 @@ class Heap:
         """Copy the heap's metadata (and optionally its superblock region) to
         host numpy arrays; see ``kma_b200.inspect``."""
         from .inspect import HeapImage
-        cls = np.zeros(self.nshards * 16, np.uint32)
+        cls = np.zeros(self.cls_lines, np.uint32)
         state = np.zeros(self.sblocks, np.uint32)
         fl = np.zeros(self.sblocks, np.uint32)
         fl_len = np.zeros(1, np.uint64)
@@ -144,7 +145,7 @@ class Heap:
         freelist = None if n == 2**64 - 1 else fl[:n].astype(np.int64)
         return HeapImage(sb_size_log2=self.sb_size_log2, sblocks=self.sblocks, pages=self.pages,
                          nclasses=self.nclasses, cls_size=list(self.cls_size),
-                         cls_slots=list(self.cls_slots), cls_raw=cls.reshape(self.nshards, 16),
+                         cls_slots=list(self.cls_slots), cls_raw=cls, cls_shards=list(self.cls_shards),
                          state=state, freelist=freelist, region=reg if region else None)
 
     # -- serial replay ------------------------------------------------------

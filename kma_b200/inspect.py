@@ -33,7 +33,8 @@ class HeapImage:
     nclasses: int
     cls_size: list
     cls_slots: list
-    cls_raw: np.ndarray          # (nshards, 16) raw class-table words
+    cls_raw: np.ndarray          # raw class-table words, class-major
+    cls_shards: list             # words (shards) per class
     state: np.ndarray            # (sblocks,) class<<28 | slots<<14 | free
     freelist: np.ndarray | None  # FIFO order; None if the list has a cycle
     region: np.ndarray | None = None
@@ -51,10 +52,12 @@ class Canonical:
 
 
 def decode(img: HeapImage) -> Canonical:
-    raw = np.asarray(img.cls_raw, np.int64).reshape(-1, 16)[:, : img.nclasses]
+    raw = np.asarray(img.cls_raw, np.int64).reshape(-1)
     cls = np.full(img.nclasses, -1, np.int64)
+    base = 0
     for c in range(img.nclasses):
-        col = raw[:, c]
+        col = raw[base:base + img.cls_shards[c]]
+        base += img.cls_shards[c]
         nz = col[col != 0]
         if len(nz) > 1:
             cls[c] = -3

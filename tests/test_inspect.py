@@ -19,7 +19,8 @@ def image_from_port(p, sblocks, log2, ops, out):
     for c, v in enumerate(d["cls"]):
         cls[0, c] = 0 if v == -1 else 1 if v == -2 else v + 2
     img = ins.HeapImage(log2, sblocks, sblocks - 1, log2 - 1, sizes,
-                        oracle.port_tables(log2)[1], cls, st, d["freelist"].copy(), p.region())
+                        oracle.port_tables(log2)[1], cls.reshape(-1)[: log2 - 1], [1] * (log2 - 1), st,
+                        d["freelist"].copy(), p.region())
     return img, d
 
 
