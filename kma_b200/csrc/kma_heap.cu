@@ -241,17 +241,23 @@ extern "C" int kma_create_ex(const kma_config *cfg, void *stream, kma_heap_t *ou
 	 * header, i.e. sblocks - 1 superblocks enter the free list */
 	k->hh.pages = (uint32_t)nsb - 1;
 	const bool compat = cfg->flags & KMA_CFG_COMPAT;
-	/* shards per class: a budget of pinned current superblocks of pages/32
-	 * (about 3% of the heap if every shard of every class held one),
-	 * divided among the classes in inverse proportion to their slots, at
-	 * most cfg->shards (default KMA_MAX_SHARDS) per class */
+	/* shards per class.  Two pressures: every reservation of a class CASes
+	 * its shard's current superblock state, so each class needs enough
+	 * shards to spread the warps (a base of pages/1024, at most 64); and a
+	 * class with few slots per superblock refills that many times more
+	 * often, so it gets pages/32/slots shards if that is more.  At most
+	 * cfg->shards (default KMA_MAX_SHARDS) per class; pinned current
+	 * superblocks stay near 3% of the heap. */
 	uint32_t cap = compat ? 1u : (cfg->shards ? cfg->shards : KMA_MAX_SHARDS);
 	uint32_t budget = k->hh.pages / 32;
+	uint32_t base_sh = k->hh.pages / 1024;
+	base_sh = base_sh > 64 ? 64 : base_sh;
 	uint32_t lines = 0;
 	for (uint32_t c = 0; c < KMA_MAX_CLASSES; c++) {
 		uint32_t n = 0;
 		if (c < k->hh.nclasses) {
 			n = budget / k->hh.cls_slots[c];
+			n = n < base_sh ? base_sh : n;
 			n = n < 1 ? 1 : n > cap ? cap : n;
 		}
 		k->hh.cls_nsh[c] = n;
