@@ -174,6 +174,31 @@ int kma_wl_serial(kma_wl_t w, uint32_t nrounds, int round_major, int mode, void 
  * Synchronous on `stream`; pinned host buffers make the copies async. */
 int kma_wl_run_host(kma_wl_t w, const uint64_t *seeds_host, uint32_t nrounds, int mode,
 		uint64_t *hashes_host, kma_wl_stats *stats, void *stream);
+/* Allocation-free run.  No counterpart in the reference.  For hosts that
+ * must not call cudaMalloc/cudaFree while they run a batch -- those calls
+ * synchronise with the whole device, stalling every other stream a serving
+ * loop keeps busy, and a host framework with its own caching allocator may
+ * own the memory budget so that a private allocation fails -- this runs
+ * the same workload as kma_wl_run_host (reset the heap, seed item g with
+ * seeds_dev[g], `nrounds` rounds, drain; `serial` != 0 runs one thread,
+ * round by round, like kma_wl_serial) without a kma_wl handle: the
+ * per-item scratch (PRNG, live-block table, counters) lives in a fixed
+ * KMA_WL_NOALLOC_SCRATCH_BYTES array inside the library, which every GPU
+ * that loads the library holds until the process exits.  Inputs and
+ * outputs are the caller's device memory: seeds_dev[items] in,
+ * hashes_dev[items] (each item's ordered malloc hash) and *stats_dev out.
+ * It allocates nothing.  items > KMA_WL_NOALLOC_MAX_ITEMS returns
+ * KMA_EINVAL.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make that first call before any
+ * stream capture.  Every call reuses the same array (each call clears
+ * what must start at zero): calls that overlap on the GPU, on any stream,
+ * race and corrupt each other.  Stream-ordered; returns before the work
+ * completes. */
+#define KMA_WL_NOALLOC_MAX_ITEMS 8192
+#define KMA_WL_NOALLOC_SCRATCH_BYTES (4u << 20)
+int kma_wl_run_noalloc(kma_heap_t h, int program, uint64_t items, const uint64_t *seeds_dev,
+		uint32_t nrounds, int mode, int serial, uint64_t *hashes_dev, kma_wl_stats *stats_dev,
+		void *stream);
 /* Counters to host (synchronises the stream). */
 int kma_wl_stats_get(kma_wl_t w, void *stream, kma_wl_stats *out);
 /* Per-item ordered malloc hashes (device pointer, items x u64). */

@@ -89,6 +89,8 @@ SIGNATURES = [
     ("kma_wl_serial", c_int, [c_void_p, c_uint32, c_int, c_int, c_void_p]),
     ("kma_wl_run_host", c_int, [c_void_p, c_void_p, c_uint32, c_int, c_void_p,
                                 POINTER(KmaWlStats), c_void_p]),
+    ("kma_wl_run_noalloc", c_int, [c_void_p, c_int, c_uint64, c_void_p, c_uint32, c_int, c_int,
+                                   c_void_p, c_void_p, c_void_p]),
     ("kma_wl_stats_get", c_int, [c_void_p, c_void_p, POINTER(KmaWlStats)]),
     ("kma_wl_item_hashes", c_void_p, [c_void_p]),
     ("kma_wl_live", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),

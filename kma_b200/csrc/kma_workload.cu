@@ -22,6 +22,7 @@
  */
 #include <string.h>
 #include <stdlib.h>
+#include <mutex>
 #include "kma_internal.h"
 
 #define WL_CAP 32
@@ -698,4 +699,150 @@ extern "C" int kma_bench_atomics(int distinct, uint64_t threads, uint32_t iters,
 	cudaEventDestroy(e1);
 	cudaFree(buf);
 	return rc;
+}
+
+/* ------------------------------------------------------------------ */
+/* allocation-free workload run (kma_wl_run_noalloc)                   */
+/* ------------------------------------------------------------------ */
+/* Some hosts cannot call cudaMalloc when they run a batch: cudaMalloc and
+ * cudaFree synchronise with the whole device (stalling every other stream
+ * a serving loop keeps busy), and a host framework with its own caching
+ * allocator (PyTorch's, say) may own the device memory budget so that a
+ * private cudaMalloc fails or fragments its pool.  For them this entry
+ * point runs the workload on scratch that lives in this file-scope array
+ * instead of the kma_wl handle's cudaMalloc'd scratch.  The array is part
+ * of the library's device image: every GPU that loads the library holds
+ * its 4 MiB until the process exits, and every call shares it. */
+static __device__ __align__(256) unsigned char kma_noalloc_scratch[KMA_WL_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+/* Device address of kma_noalloc_scratch per device.  In host code the
+ * array's name is only a host-side stand-in, so the address comes from
+ * cudaGetSymbolAddress, once per device, with that device current. */
+struct noalloc_slot {
+	void *ptr;
+	bool ready;
+};
+std::mutex g_noalloc_mu;
+noalloc_slot g_noalloc[256];
+
+int noalloc_scratch(int dev, unsigned char **out)
+{
+	if (dev < 0 || dev >= 256)
+		return KMA_ENODEV;
+	std::lock_guard<std::mutex> lk(g_noalloc_mu);
+	if (!g_noalloc[dev].ready) {
+		void *p = NULL;
+		if (cudaGetSymbolAddress(&p, kma_noalloc_scratch) != cudaSuccess || !p) {
+			cudaGetLastError();
+			return KMA_ECUDA;
+		}
+		g_noalloc[dev].ptr = p;
+		g_noalloc[dev].ready = true;
+	}
+	*out = (unsigned char *)g_noalloc[dev].ptr;
+	return KMA_OK;
+}
+
+size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+/* Counters and the XOR of the per-item hashes into the caller's
+ * kma_wl_stats (one block). */
+__global__ void k_noalloc_finish(const unsigned long long *stats, const uint64_t *hash, uint64_t items,
+		kma_wl_stats *out)
+{
+	__shared__ unsigned long long part[32];
+	uint64_t x = 0;
+	for (uint64_t g = threadIdx.x; g < items; g += blockDim.x)
+		x ^= hash[g];
+	uint32_t lo = __reduce_xor_sync(0xffffffffu, (uint32_t)x);
+	uint32_t hi = __reduce_xor_sync(0xffffffffu, (uint32_t)(x >> 32));
+	if ((threadIdx.x & 31) == 0)
+		part[threadIdx.x / 32] = ((unsigned long long)hi << 32) | lo;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		unsigned long long h = 0;
+		for (uint32_t i = 0; i < blockDim.x / 32; i++)
+			h ^= part[i];
+		out->mallocs = stats[0];
+		out->frees = stats[1];
+		out->nulls = stats[2];
+		out->bad_tags = stats[3];
+		out->offset_hash = h;
+		out->fill_bytes = stats[4];
+		out->verify_bytes = stats[5];
+	}
+}
+
+} /* namespace */
+
+extern "C" int kma_wl_run_noalloc(kma_heap_t h, int program, uint64_t items, const uint64_t *seeds_dev,
+		uint32_t nrounds, int mode, int serial, uint64_t *hashes_dev, kma_wl_stats *stats_dev,
+		void *stream)
+{
+	if (!h || !seeds_dev || !hashes_dev || !stats_dev || items == 0)
+		return KMA_EINVAL;
+	if (items > KMA_WL_NOALLOC_MAX_ITEMS)
+		return KMA_EINVAL; /* the fixed scratch holds at most this many items */
+	if (program != KMA_WL_C1 && program != KMA_WL_C2)
+		return KMA_EINVAL;
+	if (mode != KMA_MODE_PLAIN && mode != KMA_MODE_WARP)
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	if (!g.ok)
+		return KMA_ENODEV;
+	unsigned char *base = NULL;
+	int rc = noalloc_scratch(h->device, &base);
+	if (rc != KMA_OK)
+		return rc;
+	size_t n = (size_t)items;
+	size_t o_rng = 0;
+	size_t o_nlive = up256(o_rng + 8 * n);
+	size_t o_loff = up256(o_nlive + 4 * n);
+	size_t o_lsize = up256(o_loff + 8 * n * WL_CAP);
+	size_t o_stats = up256(o_lsize + 4 * n * WL_CAP);
+	if (o_stats + 64 > sizeof(kma_noalloc_scratch))
+		return KMA_EINVAL;
+	wl_dev d;
+	d.items = items;
+	d.program = program;
+	d.rng = (uint64_t *)(base + o_rng);
+	d.hash = hashes_dev; /* the per-item hashes are the caller's output */
+	d.nlive = (uint32_t *)(base + o_nlive);
+	d.live_off = (unsigned long long *)(base + o_loff);
+	d.live_size = (uint32_t *)(base + o_lsize);
+	d.stats = (unsigned long long *)(base + o_stats);
+	d.seeds = NULL;
+	cudaStream_t st = kma_stream(stream);
+	rc = kma_reset(h, stream);
+	if (rc != KMA_OK)
+		return rc;
+	/* k_wl_begin clears what must start at zero: each item's hash and live
+	 * count and the counters; the array keeps the previous call's data */
+	uint32_t bb = wl_blocks(items, 256);
+	k_wl_begin<<<bb < 148 * 8 ? bb : 148 * 8, 256, 0, st>>>(d, 0, seeds_dev);
+	if (serial) {
+		if (mode == KMA_MODE_WARP)
+			k_wl_serial<KMA_MODE_WARP><<<1, 1, 0, st>>>(h->dh, d, nrounds, 1);
+		else
+			k_wl_serial<KMA_MODE_PLAIN><<<1, 1, 0, st>>>(h->dh, d, nrounds, 1);
+	} else {
+		uint32_t nb = wl_blocks(items, 256);
+		int per_sm = 0, sms = 0;
+		const void *fn = mode == KMA_MODE_WARP ? (const void *)k_wl_rounds<KMA_MODE_WARP>
+						       : (const void *)k_wl_rounds<KMA_MODE_PLAIN>;
+		KMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
+		KMA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+		uint64_t resident = (uint64_t)(per_sm > 0 ? per_sm : 1) * (uint64_t)(sms > 0 ? sms : 1);
+		if (nb > resident)
+			nb = (uint32_t)resident;
+		if (mode == KMA_MODE_WARP)
+			k_wl_rounds<KMA_MODE_WARP><<<nb, 256, 0, st>>>(h->dh, d, nrounds, 1);
+		else
+			k_wl_rounds<KMA_MODE_PLAIN><<<nb, 256, 0, st>>>(h->dh, d, nrounds, 1);
+	}
+	k_noalloc_finish<<<1, 1024, 0, st>>>(d.stats, hashes_dev, items, stats_dev);
+	KMA_CUDA(cudaGetLastError());
+	return KMA_OK;
 }
