@@ -230,8 +230,20 @@ def run_ours(args) -> int:
     sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
                            if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit()
                            else local)
-    step_ms, rounds_ms, clocks = timed(heap, wl, mode, args.steps, args.warmup, sampler)
+    step_ms, rounds_ms, clocks = timed(heap, wl, mode, args.steps, args.warmup,
+                                       None if args.only_timed else sampler)
     st = wl.stats(stream)
+    if args.only_timed:
+        if rank == 0:
+            print(json.dumps({"items": ITEMS, "rounds": ROUNDS, "sblocks": SBLOCKS, "mode": args.mode,
+                              "step_ms": [round(x, 3) for x in step_ms],
+                              "rounds_ms": [round(x, 3) for x in rounds_ms],
+                              "ops_per_step": st["mallocs"] + st["frees"], "nulls": st["nulls"],
+                              "bad_tags": st["bad_tags"],
+                              "rounds_launch_bytes_per_step": None}))
+        wl.close()
+        heap.close()
+        return 0
     ops_step = st["mallocs"] + st["frees"]
     total_ms = sum(step_ms)
     t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
@@ -368,6 +380,7 @@ def run_ours(args) -> int:
 
 
 def main(argv=None) -> int:
+    global ITEMS, ROUNDS, SBLOCKS
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -376,7 +389,13 @@ def main(argv=None) -> int:
     ap.add_argument("--mode", choices=["warp", "plain"], default="warp")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-kernel comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--items", type=int, default=ITEMS, help="work-items (a smaller case for ncu)")
+    ap.add_argument("--rounds", type=int, default=ROUNDS)
+    ap.add_argument("--sblocks", type=int, default=SBLOCKS, help="16 KiB superblocks in the heap")
+    ap.add_argument("--only-timed", action="store_true",
+                    help="run the timed steps only and print a short line (profiling)")
     args = ap.parse_args(argv)
+    ITEMS, ROUNDS, SBLOCKS = args.items, args.rounds, args.sblocks
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
