@@ -197,6 +197,33 @@ __device__ __forceinline__ void fence_acqrel()
 {
 	asm volatile("fence.acq_rel.gpu;" ::: "memory");
 }
+/* Relaxed forms for the hot path.  Slot claims and releases are decided by
+ * these atomics at L2, the coherence point; a claim is issued only after
+ * the reservation it depends on has returned (the GPU does not speculate),
+ * and the only plain stores another thread must see first -- a refill's
+ * bitmap zeroing and a free's word-0 residue -- are fenced before their
+ * publication (sb_format, and_release). */
+__device__ __forceinline__ uint32_t cas_relaxed(uint32_t *p, uint32_t cmp, uint32_t val)
+{
+	uint32_t old;
+	asm volatile("atom.relaxed.gpu.global.cas.b32 %0, [%1], %2, %3;"
+		     : "=r"(old) : "l"(p), "r"(cmp), "r"(val) : "memory");
+	return old;
+}
+__device__ __forceinline__ uint32_t or_relaxed(uint32_t *p, uint32_t v)
+{
+	uint32_t old;
+	asm volatile("atom.relaxed.gpu.global.or.b32 %0, [%1], %2;"
+		     : "=r"(old) : "l"(p), "r"(v) : "memory");
+	return old;
+}
+__device__ __forceinline__ uint32_t and_release(uint32_t *p, uint32_t v)
+{
+	uint32_t old;
+	asm volatile("atom.release.gpu.global.and.b32 %0, [%1], %2;"
+		     : "=r"(old) : "l"(p), "r"(v) : "memory");
+	return old;
+}
 __device__ __forceinline__ uint32_t lane_id()
 {
 	uint32_t l;
@@ -495,7 +522,7 @@ __device__ __forceinline__ void *sb_get_block(kma_heap *h, uint32_t s, uint32_t 
 		while (cand) {
 			uint32_t b = __ffs(cand) - 1;
 			uint32_t bit = 1u << b;
-			uint32_t old = or_acqrel(wp, bit);
+			uint32_t old = or_relaxed(wp, bit);
 			if (!(old & bit)) {
 				unsigned char *p = sb + KMA_SB_HDR + (size_t)(k * 32 + b) * size;
 				*reinterpret_cast<uint32_t *>(p) = hint;
@@ -526,7 +553,7 @@ __device__ inline void *kma_malloc(kma_heap *h, size_t size)
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
 		/* kma.cl:163: CAS 0 -> POISON doubles as the read of the slot */
-		uint32_t cur = cas_acqrel(clsw, 0, KMA_POISON);
+		uint32_t cur = cas_relaxed(clsw, 0, KMA_POISON);
 		if (cur == 0) {
 			/* refill, kma.cl:166-195 */
 			int64_t s = sb_dequeue(h);
@@ -551,14 +578,14 @@ __device__ inline void *kma_malloc(kma_heap *h, size_t size)
 		uint32_t s = cur - KMA_CLS_BASE;
 		uint32_t *stp = &h->sb_state[s];
 		/* kma.cl:198 reads the state with atom_add(.., 0) */
-		uint32_t st = add_acqrel(stp, 0);
+		uint32_t st = atomicAdd(stp, 0u);
 		if (st_class(st) != (uint32_t)c || st_free(st) == 0)
 			continue;
 		uint32_t fr = st_free(st) - 1;
-		if (cas_acqrel(stp, st, st - 1) != st)
+		if (cas_relaxed(stp, st, st - 1) != st)
 			continue;
 		if (fr == 0)
-			cas_acqrel(clsw, cur, 0); /* kma.cl:216-218 */
+			cas_relaxed(clsw, cur, 0); /* kma.cl:216-218 */
 		return sb_get_block(h, s, c, fr);
 	}
 	set_err(h, KMA_ERR_TIMEOUT);
@@ -588,7 +615,7 @@ __device__ __forceinline__ bool block_locate(const kma_heap *h, const void *p, u
 __device__ __forceinline__ void sb_recycle(kma_heap *h, uint32_t s, uint32_t c)
 {
 	uint32_t home = h->sb_home[s];
-	cas_acqrel(cls_word(h, c, home), s + KMA_CLS_BASE, 0);
+	cas_relaxed(cls_word(h, c, home), s + KMA_CLS_BASE, 0);
 	sb_enqueue(h, s);
 }
 } /* namespace kma_detail */
@@ -606,24 +633,33 @@ __device__ inline void kma_free(kma_heap *h, void *p)
 	}
 	unsigned char *sb = sb_addr(h, s);
 	uint32_t bit = 1u << (slot & 31);
-	/* kma.cl:336-338: the old bitmap word lands in word 0 of the block */
-	uint32_t old = and_acqrel(bitmap_word(h, sb, slot >> 5), ~bit);
-	*reinterpret_cast<volatile uint32_t *>(p) = old;
-	if (!(old & bit)) {
+	uint32_t *wp = bitmap_word(h, sb, slot >> 5);
+	/* kma.cl:336-338 leaves the bitmap word as it was before the clear in
+	 * word 0 of the block, but stores it after the clear: by then another
+	 * thread may already own the slot and have written that word.  Store
+	 * the same value first, then clear the bit with release semantics. */
+	uint32_t cur = ld_relaxed(wp);
+	if (!(cur & bit)) {
 		/* double free: the reference increments the free count anyway
 		 * and corrupts the superblock (kma.cl:333-335); refuse it */
 		set_err(h, KMA_ERR_BADFREE);
 		return;
 	}
+	*reinterpret_cast<volatile uint32_t *>(p) = cur;
+	uint32_t old = and_release(wp, ~bit);
+	if (!(old & bit)) {
+		set_err(h, KMA_ERR_BADFREE); /* a concurrent double free */
+		return;
+	}
 	uint32_t *stp = &h->sb_state[s];
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
-		uint32_t st = add_acqrel(stp, 0); /* kma.cl:343 */
+		uint32_t st = atomicAdd(stp, 0u); /* kma.cl:343 */
 		uint32_t slots = st_slots(st);
 		uint32_t fr = st_free(st) + 1;
 		bool enq = fr == slots;
 		uint32_t nst = st_make(st_class(st), slots, enq ? 0 : fr);
-		if (cas_acqrel(stp, st, nst) == st) {
+		if (cas_relaxed(stp, st, nst) == st) {
 			if (enq)
 				sb_recycle(h, s, c);
 			return;
@@ -680,9 +716,9 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 	uint32_t *clsw = cls_word(h, c, shard);
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
-		uint32_t cur = ld_acquire(clsw);
+		uint32_t cur = ld_relaxed(clsw);
 		if (cur == 0) {
-			if (cas_acqrel(clsw, 0, KMA_POISON) != 0)
+			if (cas_relaxed(clsw, 0, KMA_POISON) != 0)
 				continue;
 			int64_t s = sb_dequeue(h);
 			if (s < 0) {
@@ -716,10 +752,10 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		}
 		uint32_t fr = st_free(st);
 		uint32_t t = want < fr ? want : fr;
-		if (cas_acqrel(stp, st, st - t) != st)
+		if (cas_relaxed(stp, st, st - t) != st)
 			continue;
 		if (fr == t)
-			cas_acqrel(clsw, cur, 0);
+			cas_relaxed(clsw, cur, 0);
 		r.sb = s;
 		r.cls = c;
 		r.left = t;
@@ -766,7 +802,7 @@ __device__ __forceinline__ uint32_t warp_claim_step(kma_heap *h, warp_resv &r, u
 	}
 	uint32_t got = 0;
 	if (pick) {
-		uint32_t old = or_acqrel(wp, pick);
+		uint32_t old = or_relaxed(wp, pick);
 		got = pick & ~old;
 	}
 	r.left -= __popc(got);
@@ -879,16 +915,23 @@ __device__ inline void kma_free_warp(kma_heap *h, void *p)
 	uint32_t bit = valid ? (1u << (slot & 31)) : 0u;
 	uint32_t mask = __reduce_or_sync(wpeers, bit);
 	uint32_t wleader = __ffs(wpeers) - 1;
+	/* word-0 residue (kma.cl:338) before the bits are released, as in
+	 * kma_free; the warp barrier orders every lane's store before the
+	 * leader's release */
+	uint32_t *wp = valid ? bitmap_word(h, sb_addr(h, s), word) : NULL;
+	if (valid) {
+		uint32_t cur = ld_relaxed(wp);
+		if (cur & bit)
+			*reinterpret_cast<volatile uint32_t *>(p) = cur;
+	}
+	__syncwarp(active);
 	uint32_t old = 0;
 	if (valid && lane == wleader)
-		old = and_acqrel(bitmap_word(h, sb_addr(h, s), word), ~mask);
+		old = and_release(wp, ~mask);
 	old = __shfl_sync(active, old, wleader);
 	bool good = valid && (old & bit);
-	if (valid) {
-		*reinterpret_cast<volatile uint32_t *>(p) = old; /* kma.cl:338 */
-		if (!good)
-			set_err(h, KMA_ERR_BADFREE); /* double free, see kma_free */
-	}
+	if (valid && !good)
+		set_err(h, KMA_ERR_BADFREE); /* double free, see kma_free */
 	/* 2) return k slots to the superblock: one state update per superblock */
 	uint32_t speers = __match_any_sync(active, good ? s : 0xffffffffu);
 	uint32_t k = __popc(speers);
@@ -902,7 +945,7 @@ __device__ inline void kma_free_warp(kma_heap *h, void *p)
 			uint32_t fr = st_free(st) + k;
 			bool enq = fr == slots;
 			uint32_t nst = st_make(st_class(st), slots, enq ? 0 : fr);
-			uint32_t seen = cas_acqrel(stp, st, nst);
+			uint32_t seen = cas_relaxed(stp, st, nst);
 			if (seen == st) {
 				if (enq)
 					sb_recycle(h, s, c);

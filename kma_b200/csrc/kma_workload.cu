@@ -294,7 +294,7 @@ __device__ __forceinline__ void flush_counters(const wl_dev &w, uint32_t mask, u
  * their rounds and pin their last live blocks while later waves start,
  * which fragments the heap far beyond what concurrent items do.) */
 template <int MODE>
-__global__ void __launch_bounds__(256) k_wl_rounds(kma_heap *h, wl_dev w, uint32_t nrounds, int drain)
+__global__ void __launch_bounds__(256, 4) k_wl_rounds(kma_heap *h, wl_dev w, uint32_t nrounds, int drain)
 {
 	const uint32_t mask = 0xffffffffu;
 	const uint32_t lane = threadIdx.x & 31;
@@ -302,28 +302,7 @@ __global__ void __launch_bounds__(256) k_wl_rounds(kma_heap *h, wl_dev w, uint32
 	const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	wl_counters ct = {0, 0, 0, 0, 0, 0};
 	const bool c2 = w.program == KMA_WL_C2;
-	if (w.items <= T) {
-		/* one item per thread: its state stays in registers */
-		uint64_t g = tid;
-		bool act = g < w.items;
-		wl_item it;
-		it.rng = act ? w.rng[g] : 0;
-		it.hash = act ? w.hash[g] : 0;
-		it.nlive = act ? w.nlive[g] : 0;
-		for (uint32_t r = 0; r < nrounds; r++) {
-			if (c2)
-				c2_round<MODE>(h, w, mask, lane, act, g, it, ct);
-			else
-				c1_round<MODE>(h, mask, lane, act, g, it, ct);
-		}
-		if (drain && c2)
-			c2_drain<MODE>(h, w, mask, lane, act, g, it, ct);
-		if (act) {
-			w.rng[g] = it.rng;
-			w.hash[g] = it.hash;
-			w.nlive[g] = it.nlive;
-		}
-	} else {
+	{
 		for (uint32_t r = 0; r <= nrounds; r++) {
 			if (r == nrounds && !(drain && c2))
 				break;
