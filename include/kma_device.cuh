@@ -684,9 +684,12 @@ __device__ inline void kma_free(kma_heap *h, void *p)
 /* ------------------------------------------------------------------ */
 namespace kma_detail {
 
-/* Leader-side state of one group's reservation. */
+/* Leader-side state of one group's reservation.  kword/known: the last
+ * bitmap word this reservation touched and its value as the atomicOr
+ * returned it (claims go blind on a word first: setting a bit that is
+ * already set changes nothing, and the returned word says what is free). */
 struct warp_resv {
-	uint32_t sb, cls, left, cursor, pre_hi, hint;
+	uint32_t sb, cls, left, cursor, pre_hi, hint, kword, known;
 	bool pre;
 };
 
@@ -711,6 +714,7 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		r.pre_hi = slots;
 		r.hint = slots - 1;
 		r.pre = true;
+		r.kword = 0xffffffffu;
 		return 1;
 	}
 	uint32_t *clsw = cls_word(h, c, shard);
@@ -737,6 +741,7 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 			r.pre_hi = slots;
 			r.hint = slots - 1;
 			r.pre = true;
+			r.kword = 0xffffffffu;
 			return 1;
 		}
 		if (cur == KMA_POISON) {
@@ -761,6 +766,7 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		r.left = t;
 		r.cursor = fr - t; /* lowest of the t serial hints fr-1 .. fr-t */
 		r.pre = false;
+		r.kword = 0xffffffffu;
 		r.hint = fr - 1;
 		return 1;
 	}
@@ -790,7 +796,9 @@ __device__ __forceinline__ uint32_t warp_claim_step(kma_heap *h, warp_resv &r, u
 	uint32_t *wp = bitmap_word(h, sb, k);
 	uint32_t words = h->cls_words[r.cls];
 	uint32_t valid = (k == words - 1 && (slots & 31)) ? ((1u << (slots & 31)) - 1u) : 0xffffffffu;
-	uint32_t v = ld_relaxed(wp);
+	/* first visit of a word: assume its bits are clear; the atomicOr's
+	 * result then says which ones really were */
+	uint32_t v = r.kword == k ? r.known : 0u;
 	uint32_t cand = ~v & valid & (0xffffffffu << lo);
 	uint32_t pick = 0;
 	/* take the lowest `left` candidate bits */
@@ -804,6 +812,8 @@ __device__ __forceinline__ uint32_t warp_claim_step(kma_heap *h, warp_resv &r, u
 	if (pick) {
 		uint32_t old = or_relaxed(wp, pick);
 		got = pick & ~old;
+		r.kword = k;
+		r.known = old | pick;
 	}
 	r.left -= __popc(got);
 	if (got == pick) {

@@ -13,12 +13,12 @@
  * The same programs, in host C, are the oracle's (oracle/workload.c);
  * serial execution of both yields identical offsets.
  *
- * Concurrent execution: one thread per item, all rounds in one launch.
- * Payload tags are written and verified warp-cooperatively (the warp
- * walks the blocks of its lanes; lane l touches words l, l+32, ...), so a
- * block's stores are coalesced instead of one lane writing it word by
- * word.  The per-item state (PRNG, ordered malloc hash, live table) lives
- * in device scratch owned by the kma_wl handle.
+ * Concurrent execution: a persistent grid walks the items round by round
+ * (k_wl_rounds).  Each lane tags and verifies its own block with 16-byte
+ * accesses unrolled by four, so a warp keeps many independent requests in
+ * flight (the verify pass is bound by memory latency, not by bandwidth).
+ * The per-item state (PRNG, ordered malloc hash, live table) lives in
+ * device scratch owned by the kma_wl handle.
  */
 #include <string.h>
 #include <stdlib.h>
@@ -69,46 +69,54 @@ __device__ __forceinline__ uint32_t c1_size(uint64_t d)
 }
 __device__ __forceinline__ uint32_t c2_size(uint64_t d) { return 8u << (uint32_t)((d >> 32) % 9); }
 
-/* Warp-cooperative tag fill of every lane's block (p may be NULL). */
+/* Tag fill of this lane's own block (p may be NULL).  Blocks start 4 bytes
+ * past a 16-byte boundary (12 + slot*size), so the head words go one at a
+ * time and the rest as 16-byte stores. */
 __device__ __forceinline__ void coop_fill(uint32_t mask, uint32_t lane, void *p, uint32_t n, uint32_t tag)
 {
-	uint32_t m = __ballot_sync(mask, p != NULL);
-	while (m) {
-		uint32_t j = __ffs(m) - 1;
-		m &= m - 1;
-		uint32_t *pj = (uint32_t *)__shfl_sync(mask, (unsigned long long)p, j);
-		uint32_t nj = __shfl_sync(mask, n, j) >> 2;
-		uint32_t tj = __shfl_sync(mask, tag, j);
-		uint32_t step = __popc(mask);
-		uint32_t r = __popc(mask & ((1u << lane) - 1u));
-		for (uint32_t w = r; w < nj; w += step)
-			pj[w] = tj;
-	}
+	(void)mask;
+	(void)lane;
+	if (!p)
+		return;
+	uint32_t *w = (uint32_t *)p;
+	uint32_t nw = n >> 2, i = 0;
+	while (i < nw && ((uintptr_t)(w + i) & 15))
+		w[i++] = tag;
+	uint32_t nv = (nw - i) >> 2;
+	uint4 *v = reinterpret_cast<uint4 *>(w + i);
+	const uint4 t4 = make_uint4(tag, tag, tag, tag);
+#pragma unroll 4
+	for (uint32_t k = 0; k < nv; k++)
+		v[k] = t4;
+	for (i += nv * 4; i < nw; i++)
+		w[i] = tag;
 }
 
-/* Warp-cooperative verify; returns true in the owner lane of a block with
- * a word that differs from its tag. */
+/* Verify this lane's own block against its tag; true if any word differs.
+ * 16-byte loads unrolled by four keep several requests in flight per lane
+ * (the loads of one lane are independent of each other). */
 __device__ __forceinline__ bool coop_verify(uint32_t mask, uint32_t lane, const void *p, uint32_t n,
 		uint32_t tag)
 {
-	uint32_t m = __ballot_sync(mask, p != NULL);
-	bool mine = false;
-	while (m) {
-		uint32_t j = __ffs(m) - 1;
-		m &= m - 1;
-		const uint32_t *pj = (const uint32_t *)__shfl_sync(mask, (unsigned long long)p, j);
-		uint32_t nj = __shfl_sync(mask, n, j) >> 2;
-		uint32_t tj = __shfl_sync(mask, tag, j);
-		uint32_t step = __popc(mask);
-		uint32_t r = __popc(mask & ((1u << lane) - 1u));
-		bool bad = false;
-		for (uint32_t w = r; w < nj; w += step)
-			bad |= pj[w] != tj;
-		bool any = __any_sync(mask, bad);
-		if (lane == j)
-			mine = any;
+	(void)mask;
+	(void)lane;
+	if (!p)
+		return false;
+	const uint32_t *w = (const uint32_t *)p;
+	uint32_t nw = n >> 2, i = 0;
+	uint32_t bad = 0;
+	while (i < nw && ((uintptr_t)(w + i) & 15))
+		bad |= w[i++] ^ tag;
+	uint32_t nv = (nw - i) >> 2;
+	const uint4 *v = reinterpret_cast<const uint4 *>(w + i);
+#pragma unroll 4
+	for (uint32_t k = 0; k < nv; k++) {
+		uint4 x = v[k];
+		bad |= (x.x ^ tag) | (x.y ^ tag) | (x.z ^ tag) | (x.w ^ tag);
 	}
-	return mine;
+	for (i += nv * 4; i < nw; i++)
+		bad |= w[i] ^ tag;
+	return bad != 0;
 }
 
 template <int MODE>
