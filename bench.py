@@ -270,6 +270,14 @@ def run_ours(args) -> int:
         faults = ins.violations(res) + len(empty) + int(st_d["bad_tags"]) + int(st["bad_tags"])
         flags = heap.error_flags(clear=True, stream=stream)
 
+        # one untimed step with per-phase cycle counters (a separate kernel
+        # instantiation): where the rounds kernel spends its warps' time
+        heap.reset(stream)
+        wl.begin(SEED, stream)
+        wl.rounds(ROUNDS, mode | 2, stream=stream)
+        cyc = wl.phase_cycles(stream)
+        tot = sum(cyc) or 1
+        phase_share = {k: round(v / tot, 4) for k, v in zip(("malloc", "fill", "verify", "free"), cyc)}
         rounds_bytes = st_r["fill_bytes"] + st_r["verify_bytes"]
         rounds_ops = st_r["mallocs"] + st_r["frees"]
         mean_rounds_s = statistics.mean(rounds_ms) / 1e3
@@ -355,6 +363,7 @@ def run_ours(args) -> int:
                        "plain_mops": round(plain, 3) if plain else None,
                        "plain_default_heap_mops": round(plain_default, 3) if plain_default else None,
                        "class_shards": heap.cls_shards,
+                       "rounds_phase_share": phase_share,
                        "warp_over_plain": round(value / world / plain, 2) if plain else None},
             "roofline": {"bound": "hbm", "kernel": "k_wl_rounds<warp>",
                          "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",

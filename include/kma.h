@@ -41,6 +41,8 @@ extern "C" {
 /* allocation modes of the workload / replay kernels */
 #define KMA_MODE_PLAIN 0     /* per-thread kma_malloc / kma_free */
 #define KMA_MODE_WARP 1      /* warp-collaborative kma_malloc_warp / kma_free_warp */
+#define KMA_MODE_PROFILE 2   /* flag for kma_wl_rounds/kma_wl_drain: also count the cycles
+			      * each warp spends per phase (kma_wl_phase_cycles) */
 
 typedef struct kma_heap_s *kma_heap_t;
 struct kma_heap; /* device-side header, see kma_device.cuh */
@@ -201,6 +203,10 @@ int kma_wl_run_noalloc(kma_heap_t h, int program, uint64_t items, const uint64_t
 		void *stream);
 /* Counters to host (synchronises the stream). */
 int kma_wl_stats_get(kma_wl_t w, void *stream, kma_wl_stats *out);
+/* Cycles summed over warps since kma_wl_begin, per phase of the C2 round,
+ * for runs launched with KMA_MODE_PROFILE: [0] malloc, [1] tag fill,
+ * [2] verify, [3] free (synchronises the stream). */
+int kma_wl_phase_cycles(kma_wl_t w, void *stream, uint64_t cycles[4]);
 /* Per-item ordered malloc hashes (device pointer, items x u64). */
 const uint64_t *kma_wl_item_hashes(kma_wl_t w);
 /* Live blocks to host: nlive[items], off[32*items] (entry i of item g at

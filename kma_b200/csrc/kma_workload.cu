@@ -119,15 +119,18 @@ __device__ __forceinline__ bool coop_verify(uint32_t mask, uint32_t lane, const 
 	return bad != 0;
 }
 
+/* MODE bit 0: warp-collaborative calls; bit 1 (KMA_MODE_PROFILE): count
+ * cycles per phase (malloc, tag fill, verify, free) -- a separate
+ * instantiation, so the timed kernels carry none of it. */
 template <int MODE>
 __device__ __forceinline__ void *wl_malloc(kma_heap *h, size_t n)
 {
-	return MODE == KMA_MODE_WARP ? kma_malloc_warp(h, n) : kma_malloc(h, n);
+	return (MODE & KMA_MODE_WARP) ? kma_malloc_warp(h, n) : kma_malloc(h, n);
 }
 template <int MODE>
 __device__ __forceinline__ void wl_free(kma_heap *h, void *p)
 {
-	if (MODE == KMA_MODE_WARP)
+	if (MODE & KMA_MODE_WARP)
 		kma_free_warp(h, p);
 	else if (p)
 		kma_free(h, p);
@@ -135,7 +138,18 @@ __device__ __forceinline__ void wl_free(kma_heap *h, void *p)
 
 struct wl_counters {
 	uint32_t mallocs, frees, nulls, bad, fill, verify;
+	unsigned long long cyc[4];
 };
+
+template <int MODE>
+__device__ __forceinline__ void phase(wl_counters &ct, int k, long long &t0)
+{
+	if (MODE & KMA_MODE_PROFILE) {
+		long long t1 = clock64();
+		ct.cyc[k] += (unsigned long long)(t1 - t0);
+		t0 = t1;
+	}
+}
 
 /* Per-item state held in registers while an item runs. */
 struct wl_item {
@@ -176,6 +190,7 @@ __device__ __forceinline__ void c2_round(kma_heap *h, const wl_dev &w, uint32_t 
 		uint64_t g, wl_item &it, wl_counters &ct)
 {
 	const uint64_t items = w.items;
+	long long t0 = (MODE & KMA_MODE_PROFILE) ? clock64() : 0;
 	uint64_t d = splitmix(it.rng);
 	uint32_t n = c2_size(d);
 	uint32_t tag = (uint32_t)g;
@@ -217,7 +232,9 @@ __device__ __forceinline__ void c2_round(kma_heap *h, const wl_dev &w, uint32_t 
 		}
 	}
 	__syncwarp(mask);
+	phase<MODE>(ct, 0, t0);
 	coop_fill(mask, lane, p, n, tag);
+	phase<MODE>(ct, 1, t0);
 	uint64_t bits = splitmix(it.rng);
 	uint32_t nl = act ? it.nlive : 0;
 	uint32_t maxl = __reduce_max_sync(mask, nl);
@@ -235,7 +252,9 @@ __device__ __forceinline__ void c2_round(kma_heap *h, const wl_dev &w, uint32_t 
 		}
 		if (coop_verify(mask, lane, q, qn, tag))
 			ct.bad++;
+		phase<MODE>(ct, 2, t0);
 		wl_free<MODE>(h, q);
+		phase<MODE>(ct, 3, t0);
 		if (q) {
 			ct.frees++;
 			ct.verify += qn;
@@ -285,6 +304,9 @@ __device__ __forceinline__ void flush_counters(const wl_dev &w, uint32_t mask, u
 	unsigned long long e = __reduce_add_sync(mask, ct.fill);
 	unsigned long long f = __reduce_add_sync(mask, ct.verify);
 	if (lane == (uint32_t)(__ffs(mask) - 1)) {
+		for (int k = 0; k < 4; k++)
+			if (ct.cyc[k])
+				atomicAdd(&w.stats[10 + k], ct.cyc[k]);
 		if (a) atomicAdd(&w.stats[0], (unsigned long long)a);
 		if (b) atomicAdd(&w.stats[1], (unsigned long long)b);
 		if (c) atomicAdd(&w.stats[2], (unsigned long long)c);
@@ -308,7 +330,7 @@ __global__ void __launch_bounds__(256, 4) k_wl_rounds(kma_heap *h, wl_dev w, uin
 	const uint32_t lane = threadIdx.x & 31;
 	const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
 	const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	wl_counters ct = {0, 0, 0, 0, 0, 0};
+	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}};
 	const bool c2 = w.program == KMA_WL_C2;
 	{
 		for (uint32_t r = 0; r <= nrounds; r++) {
@@ -345,7 +367,7 @@ __global__ void k_wl_serial(kma_heap *h, wl_dev w, uint32_t nrounds, int round_m
 	if (blockIdx.x != 0 || threadIdx.x != 0)
 		return;
 	const uint32_t mask = 1u;
-	wl_counters ct = {0, 0, 0, 0, 0, 0};
+	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}};
 	if (!round_major) {
 		for (uint64_t g = 0; g < w.items; g++) {
 			wl_item it = {w.rng[g], w.hash[g], w.nlive[g]};
@@ -393,6 +415,8 @@ __global__ void k_wl_begin(wl_dev w, uint64_t seed, const uint64_t *seeds)
 	uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (g == 0) {
 		for (int i = 0; i < 6; i++)
+			w.stats[i] = 0;
+		for (int i = 10; i < 14; i++)
 			w.stats[i] = 0;
 	}
 	for (; g < w.items; g += (uint64_t)gridDim.x * blockDim.x) {
@@ -523,7 +547,7 @@ extern "C" int kma_wl_begin_seeds(kma_wl_t w, const uint64_t *seeds, void *strea
 
 static int wl_launch(kma_wl_t w, uint32_t nrounds, int mode, uint32_t bd, int drain, void *stream)
 {
-	if (!w || (mode != KMA_MODE_PLAIN && mode != KMA_MODE_WARP))
+	if (!w || (mode & ~(KMA_MODE_WARP | KMA_MODE_PROFILE)))
 		return KMA_EINVAL;
 	if (bd == 0)
 		bd = 256;
@@ -534,17 +558,19 @@ static int wl_launch(kma_wl_t w, uint32_t nrounds, int mode, uint32_t bd, int dr
 	uint32_t nb = wl_blocks(w->d.items, bd);
 	/* persistent grid: no more blocks than stay resident on all SMs */
 	int per_sm = 0, sms = 0;
-	const void *fn = mode == KMA_MODE_WARP ? (const void *)k_wl_rounds<KMA_MODE_WARP>
-					       : (const void *)k_wl_rounds<KMA_MODE_PLAIN>;
-	KMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, (int)bd, 0));
+	const void *fns[4] = {(const void *)k_wl_rounds<0>, (const void *)k_wl_rounds<1>,
+			      (const void *)k_wl_rounds<2>, (const void *)k_wl_rounds<3>};
+	KMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fns[mode], (int)bd, 0));
 	KMA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, w->heap->device));
 	uint64_t resident = (uint64_t)(per_sm > 0 ? per_sm : 1) * (uint64_t)(sms > 0 ? sms : 1);
 	if (nb > resident)
 		nb = (uint32_t)resident;
-	if (mode == KMA_MODE_WARP)
-		k_wl_rounds<KMA_MODE_WARP><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain);
-	else
-		k_wl_rounds<KMA_MODE_PLAIN><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain);
+	switch (mode) {
+	case 0: k_wl_rounds<0><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain); break;
+	case 1: k_wl_rounds<1><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain); break;
+	case 2: k_wl_rounds<2><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain); break;
+	default: k_wl_rounds<3><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain); break;
+	}
 	KMA_CUDA(cudaGetLastError());
 	return KMA_OK;
 }
@@ -831,5 +857,16 @@ extern "C" int kma_wl_run_noalloc(kma_heap_t h, int program, uint64_t items, con
 	}
 	k_noalloc_finish<<<1, 1024, 0, st>>>(d.stats, hashes_dev, items, stats_dev);
 	KMA_CUDA(cudaGetLastError());
+	return KMA_OK;
+}
+
+extern "C" int kma_wl_phase_cycles(kma_wl_t w, void *stream, uint64_t cycles[4])
+{
+	if (!w || !cycles)
+		return KMA_EINVAL;
+	kma_device_guard g(w->heap->device);
+	cudaStream_t st = kma_stream(stream);
+	KMA_CUDA(cudaMemcpyAsync(cycles, w->d.stats + 10, 32, cudaMemcpyDeviceToHost, st));
+	KMA_CUDA(cudaStreamSynchronize(st));
 	return KMA_OK;
 }

@@ -224,6 +224,14 @@ class Workload:
                 "bad_tags": s.bad_tags, "offset_hash": s.offset_hash,
                 "fill_bytes": s.fill_bytes, "verify_bytes": s.verify_bytes}
 
+    def phase_cycles(self, stream=None) -> list:
+        """Cycles per phase [malloc, fill, verify, free] of runs launched
+        with mode | KMA_MODE_PROFILE, summed over warps."""
+        out = np.zeros(4, np.uint64)
+        check(lib().kma_wl_phase_cycles(self._w, _stream_ptr(stream), out.ctypes.data),
+              "kma_wl_phase_cycles")
+        return [int(x) for x in out]
+
     @property
     def item_hashes_ptr(self) -> int:
         return int(lib().kma_wl_item_hashes(self._w))
