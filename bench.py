@@ -188,7 +188,7 @@ def run_ours(args) -> int:
 
     mode = MODE_WARP if args.mode == "warp" else MODE_PLAIN
     stream = torch.cuda.current_stream()
-    heap = Heap(SBLOCKS, SB_LOG2, stream=stream, compat=(mode == MODE_PLAIN))
+    heap = Heap(SBLOCKS, SB_LOG2, stream=stream, compat=(mode == MODE_PLAIN), shards=args.shards)
     wl = Workload(heap, WL_C2, ITEMS)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -389,7 +389,7 @@ def run_ours(args) -> int:
 
 
 def main(argv=None) -> int:
-    global ITEMS, ROUNDS, SBLOCKS
+    global ITEMS, ROUNDS, SBLOCKS, SB_LOG2
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -400,11 +400,13 @@ def main(argv=None) -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--items", type=int, default=ITEMS, help="work-items (a smaller case for ncu)")
     ap.add_argument("--rounds", type=int, default=ROUNDS)
-    ap.add_argument("--sblocks", type=int, default=SBLOCKS, help="16 KiB superblocks in the heap")
+    ap.add_argument("--sblocks", type=int, default=SBLOCKS, help="superblocks in the heap")
+    ap.add_argument("--sb-log2", type=int, default=SB_LOG2, help="superblock size (experiments)")
+    ap.add_argument("--shards", type=int, default=0, help="most class-table shards per class")
     ap.add_argument("--only-timed", action="store_true",
                     help="run the timed steps only and print a short line (profiling)")
     args = ap.parse_args(argv)
-    ITEMS, ROUNDS, SBLOCKS = args.items, args.rounds, args.sblocks
+    ITEMS, ROUNDS, SBLOCKS, SB_LOG2 = args.items, args.rounds, args.sblocks, args.sb_log2
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
