@@ -66,6 +66,9 @@
 #define KMA_SB_HDR 12u
 #define KMA_POISON 1u
 #define KMA_CLS_BASE 2u
+/* classes with at most this many slots per superblock refill privately
+ * instead of queueing behind another warp's refill (kma_malloc_warp) */
+#define KMA_PRIVATE_REFILL_SLOTS 8u
 
 #define KMA_ST_FREE_MASK 0x3fffu
 #define KMA_ST_SLOTS_SHIFT 14
@@ -721,19 +724,35 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
 		uint32_t cur = ld_relaxed(clsw);
-		if (cur == 0) {
-			if (cas_relaxed(clsw, 0, KMA_POISON) != 0)
-				continue;
+		const bool poisoned = cur == KMA_POISON;
+		if (cur == 0 || (poisoned && slots <= KMA_PRIVATE_REFILL_SLOTS)) {
+			/* cur == 0: the reference's refill under POISON (kma.cl:166-195).
+			 * POISON on a class with few slots per superblock: the refill in
+			 * flight yields about one group's worth, so rather than queue
+			 * behind it take a fresh superblock without holding the class
+			 * slot, and publish the leftover slots only if the slot is empty
+			 * by then.  Serial execution never observes POISON. */
+			bool locked = false;
+			if (!poisoned) {
+				if (cas_relaxed(clsw, 0, KMA_POISON) != 0)
+					continue;
+				locked = true;
+			}
 			int64_t s = sb_dequeue(h);
 			if (s < 0) {
-				atomicExch(clsw, 0);
+				if (locked)
+					atomicExch(clsw, 0);
 				return 0;
 			}
 			uint32_t t = want < slots ? want : slots;
 			sb_format(h, (uint32_t)s, c, slots - t, slots - t, shard);
 			/* the refiller takes the top t slots, which are exactly the
 			 * hints slots-1 .. slots-t of t serial reservations */
-			cas_acqrel(clsw, KMA_POISON, t == slots ? 0u : (uint32_t)s + KMA_CLS_BASE);
+			uint32_t pub = t == slots ? 0u : (uint32_t)s + KMA_CLS_BASE;
+			if (locked)
+				cas_acqrel(clsw, KMA_POISON, pub);
+			else if (pub)
+				cas_acqrel(clsw, 0, pub);
 			r.sb = (uint32_t)s;
 			r.cls = c;
 			r.left = t;
@@ -744,7 +763,7 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 			r.kword = 0xffffffffu;
 			return 1;
 		}
-		if (cur == KMA_POISON) {
+		if (poisoned) {
 			backoff(it);
 			continue;
 		}
