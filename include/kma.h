@@ -56,10 +56,11 @@ typedef struct kma_config {
 	uint32_t sb_size_log2; /* 12..16: 4 KiB (the reference's KMA_SB_SIZE, kma.h:27) .. 64 KiB */
 	uint32_t spin_limit;   /* bound on every device spin; 0 = default (1<<22) */
 	int32_t device;        /* CUDA ordinal; -1 = current device */
-	uint32_t shards;       /* most class-table shards per class (1..512); a warp uses
+	uint32_t shards;       /* most class-table shards per class (1..1024); a warp uses
 				* shard (global warp id) % shards(class).  Each class gets
-				* (sblocks-1)/32/slots(class) shards, clamped to [1, shards];
-				* 0 = 512.  COMPAT forces 1 (the reference's single table) */
+				* max((sblocks-1)/64, (sblocks-1)/32/slots(class)) shards,
+				* clamped to [1, shards]; 0 = 1024.  COMPAT forces 1 (the
+				* reference's single table) */
 	uint32_t flags;        /* KMA_CFG_* */
 } kma_config;
 

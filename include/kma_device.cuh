@@ -61,8 +61,8 @@
 #include <stddef.h>
 
 #define KMA_MAX_CLASSES 16
-#define KMA_MAX_SHARDS 512     /* per class */
-#define KMA_MAX_CLS_LINES 8192 /* sum over classes */
+#define KMA_MAX_SHARDS 1024    /* per class */
+#define KMA_MAX_CLS_LINES 16384 /* sum over classes */
 #define KMA_SB_HDR 12u
 #define KMA_POISON 1u
 #define KMA_CLS_BASE 2u

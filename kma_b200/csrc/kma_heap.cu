@@ -243,15 +243,16 @@ extern "C" int kma_create_ex(const kma_config *cfg, void *stream, kma_heap_t *ou
 	const bool compat = cfg->flags & KMA_CFG_COMPAT;
 	/* shards per class.  Two pressures: every reservation of a class CASes
 	 * its shard's current superblock state, so each class needs enough
-	 * shards to spread the warps (a base of pages/1024, at most 64); and a
+	 * shards to spread the warps (a base of pages/64, measured on the
+	 * config-2 workload: ceilings of 64/256/512/1024 shards gave
+	 * 1.15/2.60/2.80/2.94 G ops/s with no NULL returns); and a
 	 * class with few slots per superblock refills that many times more
 	 * often, so it gets pages/32/slots shards if that is more.  At most
 	 * cfg->shards (default KMA_MAX_SHARDS) per class; pinned current
-	 * superblocks stay near 3% of the heap. */
+	 * superblocks stay within a few percent of the heap. */
 	uint32_t cap = compat ? 1u : (cfg->shards ? cfg->shards : KMA_MAX_SHARDS);
 	uint32_t budget = k->hh.pages / 32;
-	uint32_t base_sh = k->hh.pages / 1024;
-	base_sh = base_sh > 64 ? 64 : base_sh;
+	uint32_t base_sh = k->hh.pages / 64;
 	uint32_t lines = 0;
 	for (uint32_t c = 0; c < KMA_MAX_CLASSES; c++) {
 		uint32_t n = 0;

@@ -92,31 +92,72 @@ __device__ __forceinline__ void coop_fill(uint32_t mask, uint32_t lane, void *p,
 		w[i] = tag;
 }
 
-/* Verify this lane's own block against its tag; true if any word differs.
- * 16-byte loads unrolled by four keep several requests in flight per lane
- * (the loads of one lane are independent of each other). */
-__device__ __forceinline__ bool coop_verify(uint32_t mask, uint32_t lane, const void *p, uint32_t n,
-		uint32_t tag)
+/* Blocks of at least this many bytes are verified by the whole warp. */
+#define WL_COOP_BYTES 256u
+
+/* This lane's share of verifying block p (nw words) cooperatively: head
+ * words up to the 16-byte boundary, 16-byte vectors lane, lane+32, ...,
+ * and tail words.  Nonzero if its share differs from the tag. */
+__device__ __forceinline__ uint32_t verify_share(uint32_t lane, const uint32_t *p, uint32_t nw, uint32_t tag)
 {
-	(void)mask;
-	(void)lane;
-	if (!p)
-		return false;
-	const uint32_t *w = (const uint32_t *)p;
-	uint32_t nw = n >> 2, i = 0;
+	uint32_t head = (uint32_t)((16u - ((uintptr_t)p & 15u)) & 15u) >> 2;
+	head = head < nw ? head : nw;
+	uint32_t nv = (nw - head) >> 2;
+	uint32_t tail = nw - head - 4 * nv;
+	const uint4 *v = reinterpret_cast<const uint4 *>(p + head);
 	uint32_t bad = 0;
-	while (i < nw && ((uintptr_t)(w + i) & 15))
-		bad |= w[i++] ^ tag;
-	uint32_t nv = (nw - i) >> 2;
-	const uint4 *v = reinterpret_cast<const uint4 *>(w + i);
 #pragma unroll 4
-	for (uint32_t k = 0; k < nv; k++) {
+	for (uint32_t k = lane; k < nv; k += 32) {
 		uint4 x = v[k];
 		bad |= (x.x ^ tag) | (x.y ^ tag) | (x.z ^ tag) | (x.w ^ tag);
 	}
-	for (i += nv * 4; i < nw; i++)
-		bad |= w[i] ^ tag;
-	return bad != 0;
+	if (lane < head)
+		bad |= p[lane] ^ tag;
+	if (lane < tail)
+		bad |= p[head + 4 * nv + lane] ^ tag;
+	return bad;
+}
+
+/* Verify every lane's block (p may be NULL) against its tag; true in the
+ * owner lane of a block with a word that differs.  Small blocks: each lane
+ * reads its own with 16-byte loads unrolled by eight.  Blocks of
+ * WL_COOP_BYTES or more: the warp reads each together, up to four vectors
+ * per lane, with no synchronisation per block -- mismatches collect in a
+ * per-block bit mask reduced once at the end -- so the loads of the whole
+ * pass stay in flight instead of one block's at a time. */
+__device__ __forceinline__ bool coop_verify(uint32_t mask, uint32_t lane, const void *p, uint32_t n,
+		uint32_t tag)
+{
+	const uint32_t *w = (const uint32_t *)p;
+	const bool big = p && n >= WL_COOP_BYTES;
+	uint32_t bad = 0;
+	if (p && !big) {
+		uint32_t nw = n >> 2, i = 0;
+		while (i < nw && ((uintptr_t)(w + i) & 15))
+			bad |= w[i++] ^ tag;
+		uint32_t nv = (nw - i) >> 2;
+		const uint4 *v = reinterpret_cast<const uint4 *>(w + i);
+#pragma unroll 8
+		for (uint32_t k = 0; k < nv; k++) {
+			uint4 x = v[k];
+			bad |= (x.x ^ tag) | (x.y ^ tag) | (x.z ^ tag) | (x.w ^ tag);
+		}
+		for (i += nv * 4; i < nw; i++)
+			bad |= w[i] ^ tag;
+	}
+	uint32_t mb = __ballot_sync(mask, big);
+	uint32_t badbits = 0;
+	while (mb) {
+		uint32_t j = __ffs(mb) - 1;
+		mb &= mb - 1;
+		const uint32_t *pj = (const uint32_t *)__shfl_sync(mask, (unsigned long long)w, j);
+		uint32_t nj = __shfl_sync(mask, n, j) >> 2;
+		uint32_t tj = __shfl_sync(mask, tag, j);
+		if (verify_share(lane, pj, nj, tj))
+			badbits |= 1u << j;
+	}
+	badbits = __reduce_or_sync(mask, badbits);
+	return bad != 0 || ((badbits >> lane) & 1u);
 }
 
 /* MODE bit 0: warp-collaborative calls; bit 1 (KMA_MODE_PROFILE): count
