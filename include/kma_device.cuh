@@ -944,45 +944,48 @@ __device__ inline void kma_free_warp(kma_heap *h, void *p)
 	uint32_t bit = valid ? (1u << (slot & 31)) : 0u;
 	uint32_t mask = __reduce_or_sync(wpeers, bit);
 	uint32_t wleader = __ffs(wpeers) - 1;
-	/* word-0 residue (kma.cl:338) before the bits are released, as in
-	 * kma_free; the warp barrier orders every lane's store before the
-	 * leader's release */
 	uint32_t *wp = valid ? bitmap_word(h, sb_addr(h, s), word) : NULL;
-	if (valid) {
-		uint32_t cur = ld_relaxed(wp);
-		if (cur & bit)
-			*reinterpret_cast<volatile uint32_t *>(p) = cur;
-	}
-	__syncwarp(active);
 	uint32_t old = 0;
-	if (valid && lane == wleader)
-		old = and_release(wp, ~mask);
+	if (__popc(__ballot_sync(active, valid)) == 1) {
+		/* one block: the reference's side effect, the bitmap word as it
+		 * was before the clear, in word 0 of the block (kma.cl:338) --
+		 * stored before the release, as in kma_free.  Every call of a
+		 * one-thread-at-a-time execution takes this path. */
+		if (valid) {
+			uint32_t cur = ld_relaxed(wp);
+			if (cur & bit) {
+				*reinterpret_cast<volatile uint32_t *>(p) = cur;
+				old = and_release(wp, ~mask);
+			} else {
+				old = cur;
+			}
+		}
+	} else if (valid && lane == wleader) {
+		/* several blocks at once: freed memory has no defined contents,
+		 * so the residue (a load, a store and a fence) is skipped */
+		old = atomicAnd(wp, ~mask);
+	}
 	old = __shfl_sync(active, old, wleader);
 	bool good = valid && (old & bit);
 	if (valid && !good)
 		set_err(h, KMA_ERR_BADFREE); /* double free, see kma_free */
-	/* 2) return k slots to the superblock: one state update per superblock */
+	/* 2) return k slots to the superblock: one fetch-and-add per
+	 * superblock, after the bits are clear (a count that reaches `slots`
+	 * lets the superblock be recycled and reformatted) */
 	uint32_t speers = __match_any_sync(active, good ? s : 0xffffffffu);
 	uint32_t k = __popc(speers);
 	uint32_t sleader = __ffs(speers) - 1;
 	if (good && lane == sleader) {
 		uint32_t *stp = &h->sb_state[s];
-		uint32_t lim = h->spin_limit;
-		uint32_t st = ld_relaxed(stp);
-		for (uint32_t it = 0; it < lim; it++) {
-			uint32_t slots = st_slots(st);
-			uint32_t fr = st_free(st) + k;
-			bool enq = fr == slots;
-			uint32_t nst = st_make(st_class(st), slots, enq ? 0 : fr);
-			uint32_t seen = cas_relaxed(stp, st, nst);
-			if (seen == st) {
-				if (enq)
-					sb_recycle(h, s, c);
-				return;
-			}
-			st = seen;
+		uint32_t prev = atomicAdd(stp, k);
+		uint32_t slots = st_slots(prev);
+		if (st_free(prev) + k == slots) {
+			/* kma.cl:350-367: all free -- free count 0 and recycle, unless
+			 * a reservation got in first */
+			uint32_t full = prev + k;
+			if (cas_relaxed(stp, full, st_make(st_class(prev), slots, 0)) == full)
+				sb_recycle(h, s, c);
 		}
-		set_err(h, KMA_ERR_TIMEOUT);
 	}
 }
 

@@ -278,18 +278,20 @@ __device__ __forceinline__ void c2_round(kma_heap *h, const wl_dev &w, uint32_t 
 	phase<MODE>(ct, 1, t0);
 	uint64_t bits = splitmix(it.rng);
 	uint32_t nl = act ? it.nlive : 0;
-	uint32_t maxl = __reduce_max_sync(mask, nl);
-	uint32_t j = 0;
-	for (uint32_t i = 0; i < maxl; i++) {
+	/* live entry i is freed this round when bit i of the draw is set; the
+	 * warp makes one pass per freed block of its busiest lane, each lane
+	 * freeing its entries in increasing i */
+	uint32_t fmask = nl ? ((uint32_t)bits & (nl >= 32 ? 0xffffffffu : ((1u << nl) - 1u))) : 0u;
+	uint32_t npass = __reduce_max_sync(mask, (uint32_t)__popc(fmask));
+	uint32_t rest = fmask;
+	for (uint32_t pass = 0; pass < npass; pass++) {
 		void *q = NULL;
 		uint32_t qn = 0;
-		unsigned long long qo = 0;
-		bool live = i < nl;
-		if (live) {
-			qo = w.live_off[(uint64_t)i * items + g];
+		if (rest) {
+			uint32_t i = __ffs(rest) - 1;
+			rest &= rest - 1;
+			q = h->sb_base + w.live_off[(uint64_t)i * items + g];
 			qn = w.live_size[(uint64_t)i * items + g];
-			if ((bits >> i) & 1)
-				q = h->sb_base + qo;
 		}
 		if (coop_verify(mask, lane, q, qn, tag))
 			ct.bad++;
@@ -299,16 +301,22 @@ __device__ __forceinline__ void c2_round(kma_heap *h, const wl_dev &w, uint32_t 
 		if (q) {
 			ct.frees++;
 			ct.verify += qn;
-		} else if (live) {
+		}
+	}
+	if (fmask) {
+		/* keep the survivors, in order */
+		uint32_t j = 0;
+		for (uint32_t i = 0; i < nl; i++) {
+			if ((fmask >> i) & 1)
+				continue;
 			if (j != i) {
-				w.live_off[(uint64_t)j * items + g] = qo;
-				w.live_size[(uint64_t)j * items + g] = qn;
+				w.live_off[(uint64_t)j * items + g] = w.live_off[(uint64_t)i * items + g];
+				w.live_size[(uint64_t)j * items + g] = w.live_size[(uint64_t)i * items + g];
 			}
 			j++;
 		}
-	}
-	if (act)
 		it.nlive = j;
+	}
 }
 
 template <int MODE>
