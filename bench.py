@@ -276,6 +276,7 @@ def run_ours(args) -> int:
         wl.begin(SEED, stream)
         wl.rounds(ROUNDS, mode | 2, stream=stream)
         cyc = wl.phase_cycles(stream)
+        tally = wl.tally(stream)
         tot = sum(cyc) or 1
         phase_share = {k: round(v / tot, 4) for k, v in zip(("malloc", "fill", "verify", "free"), cyc)}
         rounds_bytes = st_r["fill_bytes"] + st_r["verify_bytes"]
@@ -364,6 +365,7 @@ def run_ours(args) -> int:
                        "plain_default_heap_mops": round(plain_default, 3) if plain_default else None,
                        "class_shards": heap.cls_shards,
                        "rounds_phase_share": phase_share,
+                       "malloc_tally": tally,
                        "warp_over_plain": round(value / world / plain, 2) if plain else None},
             "roofline": {"bound": "hbm", "kernel": "k_wl_rounds<warp>",
                          "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",

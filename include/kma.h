@@ -208,6 +208,11 @@ int kma_wl_stats_get(kma_wl_t w, void *stream, kma_wl_stats *out);
  * for runs launched with KMA_MODE_PROFILE: [0] malloc, [1] tag fill,
  * [2] verify, [3] free (synchronises the stream). */
 int kma_wl_phase_cycles(kma_wl_t w, void *stream, uint64_t cycles[4]);
+/* Event counts of kma_malloc_warp in KMA_MODE_PROFILE runs since
+ * kma_wl_begin, indexed by KMA_T_* of kma_device.cuh (leader turns,
+ * reservation attempts, POISON waits, stale slots, lost CASes, refills,
+ * claim steps, empty claim steps). */
+int kma_wl_tally(kma_wl_t w, void *stream, uint64_t counts[8]);
 /* Per-item ordered malloc hashes (device pointer, items x u64). */
 const uint64_t *kma_wl_item_hashes(kma_wl_t w);
 /* Live blocks to host: nlive[items], off[32*items] (entry i of item g at

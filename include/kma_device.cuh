@@ -687,6 +687,31 @@ __device__ inline void kma_free(kma_heap *h, void *p)
 /* ------------------------------------------------------------------ */
 namespace kma_detail {
 
+} /* namespace kma_detail */
+
+/* Optional event counts of the warp-collaborative calls (diagnostics):
+ * pass a pointer to a per-thread tally to kma_malloc_warp/kma_free_warp;
+ * with the default null pointer the counting compiles away. */
+struct kma_tally {
+	uint32_t n[8];
+};
+#define KMA_T_ITER 0      /* leader turns in kma_malloc_warp */
+#define KMA_T_TRY 1       /* reservation attempts */
+#define KMA_T_POISON 2    /* waits on a refill in progress */
+#define KMA_T_STALE 3     /* class slot pointing at a full or stale superblock */
+#define KMA_T_CASFAIL 4   /* lost reservation CASes */
+#define KMA_T_REFILL 5    /* superblocks taken from the free list */
+#define KMA_T_CLAIM 6     /* bitmap claim steps */
+#define KMA_T_EMPTY 7     /* claim steps that got no bit */
+
+namespace kma_detail {
+
+__device__ __forceinline__ void tally(kma_tally *t, int k)
+{
+	if (t)
+		t->n[k]++;
+}
+
 /* Leader-side state of one group's reservation.  kword/known: the last
  * bitmap word this reservation touched and its value as the atomicOr
  * returned it (claims go blind on a word first: setting a bit that is
@@ -699,13 +724,15 @@ struct warp_resv {
 /* Reserve up to `want` slots of class c.  On success fills r (sb, left =
  * number reserved, cursor = first slot to scan from, hint) and returns 1;
  * returns 0 when the heap is exhausted or a spin expired. */
-__device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t want, warp_resv &r)
+__device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t want, warp_resv &r,
+		kma_tally *tl)
 {
 	uint32_t slots = h->cls_slots[c];
 	uint32_t shard = my_shard(h, c);
 	if (want >= slots && slots > 1) {
 		/* the group fills a whole superblock: take a fresh one privately
 		 * (it would be detached at once anyway) */
+		tally(tl, KMA_T_REFILL);
 		int64_t s = sb_dequeue(h);
 		if (s < 0)
 			return 0;
@@ -723,6 +750,7 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 	uint32_t *clsw = cls_word(h, c, shard);
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
+		tally(tl, KMA_T_TRY);
 		uint32_t cur = ld_relaxed(clsw);
 		const bool poisoned = cur == KMA_POISON;
 		if (cur == 0 || (poisoned && slots <= KMA_PRIVATE_REFILL_SLOTS)) {
@@ -738,6 +766,7 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 					continue;
 				locked = true;
 			}
+			tally(tl, KMA_T_REFILL);
 			int64_t s = sb_dequeue(h);
 			if (s < 0) {
 				if (locked)
@@ -764,6 +793,7 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 			return 1;
 		}
 		if (poisoned) {
+			tally(tl, KMA_T_POISON);
 			backoff(it);
 			continue;
 		}
@@ -771,13 +801,16 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		uint32_t *stp = &h->sb_state[s];
 		uint32_t st = ld_relaxed(stp);
 		if (st_class(st) != c || st_free(st) == 0) {
+			tally(tl, KMA_T_STALE);
 			backoff(it);
 			continue;
 		}
 		uint32_t fr = st_free(st);
 		uint32_t t = want < fr ? want : fr;
-		if (cas_relaxed(stp, st, st - t) != st)
+		if (cas_relaxed(stp, st, st - t) != st) {
+			tally(tl, KMA_T_CASFAIL);
 			continue;
+		}
 		if (fr == t)
 			cas_relaxed(clsw, cur, 0);
 		r.sb = s;
@@ -848,7 +881,7 @@ __device__ __forceinline__ uint32_t warp_claim_step(kma_heap *h, warp_resv &r, u
 
 } /* namespace kma_detail */
 
-__device__ inline void *kma_malloc_warp(kma_heap *h, size_t size)
+__device__ inline void *kma_malloc_warp(kma_heap *h, size_t size, kma_tally *tl = nullptr)
 {
 	using namespace kma_detail;
 	const uint32_t active = __activemask();
@@ -881,14 +914,18 @@ __device__ inline void *kma_malloc_warp(kma_heap *h, size_t size)
 		}
 		uint32_t bsb = 0, bword = 0, bgot = 0, bbase = 0, bhint = 0, bfail = 0;
 		if (lane == leader && c >= 0 && served < gsize && !failed) {
+			tally(tl, KMA_T_ITER);
 			if (r.left == 0) {
-				if (!warp_reserve(h, (uint32_t)c, gsize - served, r))
+				if (!warp_reserve(h, (uint32_t)c, gsize - served, r, tl))
 					failed = true;
 			}
 			if (!failed) {
 				uint32_t w;
 				uint32_t hint0 = r.hint;
 				uint32_t got = warp_claim_step(h, r, w);
+				tally(tl, KMA_T_CLAIM);
+				if (!got)
+					tally(tl, KMA_T_EMPTY);
 				bsb = r.sb;
 				bword = w;
 				bgot = got;

@@ -94,6 +94,7 @@ SIGNATURES = [
     ("kma_wl_stats_get", c_int, [c_void_p, c_void_p, POINTER(KmaWlStats)]),
     ("kma_wl_item_hashes", c_void_p, [c_void_p]),
     ("kma_wl_phase_cycles", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("kma_wl_tally", c_int, [c_void_p, c_void_p, c_void_p]),
     ("kma_wl_live", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("kma_debug_set_class_word", c_int, [c_void_p, c_uint32, c_uint32, c_void_p]),
     ("kma_bench_atomics", c_int, [c_int, c_uint64, c_uint32, c_uint32, c_void_p, POINTER(c_float)]),

@@ -164,9 +164,10 @@ __device__ __forceinline__ bool coop_verify(uint32_t mask, uint32_t lane, const 
  * cycles per phase (malloc, tag fill, verify, free) -- a separate
  * instantiation, so the timed kernels carry none of it. */
 template <int MODE>
-__device__ __forceinline__ void *wl_malloc(kma_heap *h, size_t n)
+__device__ __forceinline__ void *wl_malloc(kma_heap *h, size_t n, kma_tally *tl)
 {
-	return (MODE & KMA_MODE_WARP) ? kma_malloc_warp(h, n) : kma_malloc(h, n);
+	return (MODE & KMA_MODE_WARP) ? kma_malloc_warp(h, n, (MODE & KMA_MODE_PROFILE) ? tl : nullptr)
+				      : kma_malloc(h, n);
 }
 template <int MODE>
 __device__ __forceinline__ void wl_free(kma_heap *h, void *p)
@@ -180,6 +181,7 @@ __device__ __forceinline__ void wl_free(kma_heap *h, void *p)
 struct wl_counters {
 	uint32_t mallocs, frees, nulls, bad, fill, verify;
 	unsigned long long cyc[4];
+	kma_tally tl;
 };
 
 template <int MODE>
@@ -207,7 +209,7 @@ __device__ __forceinline__ void c1_round(kma_heap *h, uint32_t mask, uint32_t la
 	uint32_t n = c1_size(d);
 	void *p = NULL;
 	if (act) {
-		p = wl_malloc<MODE>(h, n);
+		p = wl_malloc<MODE>(h, n, &ct.tl);
 		ct.mallocs++;
 		it.hash = hash_step(it.hash, p ? (int64_t)((unsigned char *)p - h->sb_base) : -1);
 		if (!p)
@@ -259,7 +261,7 @@ __device__ __forceinline__ void c2_round(kma_heap *h, const wl_dev &w, uint32_t 
 	}
 	void *p = NULL;
 	if (act) {
-		p = wl_malloc<MODE>(h, n);
+		p = wl_malloc<MODE>(h, n, &ct.tl);
 		ct.mallocs++;
 		int64_t off = p ? (int64_t)((unsigned char *)p - h->sb_base) : -1;
 		it.hash = hash_step(it.hash, off);
@@ -356,6 +358,13 @@ __device__ __forceinline__ void flush_counters(const wl_dev &w, uint32_t mask, u
 		for (int k = 0; k < 4; k++)
 			if (ct.cyc[k])
 				atomicAdd(&w.stats[10 + k], ct.cyc[k]);
+	}
+	for (int k = 0; k < 8; k++) {
+		uint32_t v = __reduce_add_sync(mask, ct.tl.n[k]);
+		if (v && lane == (uint32_t)(__ffs(mask) - 1))
+			atomicAdd(&w.stats[16 + k], (unsigned long long)v);
+	}
+	if (lane == (uint32_t)(__ffs(mask) - 1)) {
 		if (a) atomicAdd(&w.stats[0], (unsigned long long)a);
 		if (b) atomicAdd(&w.stats[1], (unsigned long long)b);
 		if (c) atomicAdd(&w.stats[2], (unsigned long long)c);
@@ -379,7 +388,7 @@ __global__ void __launch_bounds__(256, 4) k_wl_rounds(kma_heap *h, wl_dev w, uin
 	const uint32_t lane = threadIdx.x & 31;
 	const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
 	const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}};
+	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}, {{0, 0, 0, 0, 0, 0, 0, 0}}};
 	const bool c2 = w.program == KMA_WL_C2;
 	{
 		for (uint32_t r = 0; r <= nrounds; r++) {
@@ -416,7 +425,7 @@ __global__ void k_wl_serial(kma_heap *h, wl_dev w, uint32_t nrounds, int round_m
 	if (blockIdx.x != 0 || threadIdx.x != 0)
 		return;
 	const uint32_t mask = 1u;
-	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}};
+	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}, {{0, 0, 0, 0, 0, 0, 0, 0}}};
 	if (!round_major) {
 		for (uint64_t g = 0; g < w.items; g++) {
 			wl_item it = {w.rng[g], w.hash[g], w.nlive[g]};
@@ -465,7 +474,7 @@ __global__ void k_wl_begin(wl_dev w, uint64_t seed, const uint64_t *seeds)
 	if (g == 0) {
 		for (int i = 0; i < 6; i++)
 			w.stats[i] = 0;
-		for (int i = 10; i < 14; i++)
+		for (int i = 10; i < 24; i++)
 			w.stats[i] = 0;
 	}
 	for (; g < w.items; g += (uint64_t)gridDim.x * blockDim.x) {
@@ -916,6 +925,17 @@ extern "C" int kma_wl_phase_cycles(kma_wl_t w, void *stream, uint64_t cycles[4])
 	kma_device_guard g(w->heap->device);
 	cudaStream_t st = kma_stream(stream);
 	KMA_CUDA(cudaMemcpyAsync(cycles, w->d.stats + 10, 32, cudaMemcpyDeviceToHost, st));
+	KMA_CUDA(cudaStreamSynchronize(st));
+	return KMA_OK;
+}
+
+extern "C" int kma_wl_tally(kma_wl_t w, void *stream, uint64_t counts[8])
+{
+	if (!w || !counts)
+		return KMA_EINVAL;
+	kma_device_guard g(w->heap->device);
+	cudaStream_t st = kma_stream(stream);
+	KMA_CUDA(cudaMemcpyAsync(counts, w->d.stats + 16, 64, cudaMemcpyDeviceToHost, st));
 	KMA_CUDA(cudaStreamSynchronize(st));
 	return KMA_OK;
 }

@@ -232,6 +232,14 @@ class Workload:
               "kma_wl_phase_cycles")
         return [int(x) for x in out]
 
+    def tally(self, stream=None) -> dict:
+        """kma_malloc_warp event counts of KMA_MODE_PROFILE runs."""
+        out = np.zeros(8, np.uint64)
+        check(lib().kma_wl_tally(self._w, _stream_ptr(stream), out.ctypes.data), "kma_wl_tally")
+        names = ("turns", "tries", "poison_waits", "stale", "cas_lost", "refills", "claims",
+                 "empty_claims")
+        return {k: int(v) for k, v in zip(names, out)}
+
     @property
     def item_hashes_ptr(self) -> int:
         return int(lib().kma_wl_item_hashes(self._w))
