@@ -220,6 +220,30 @@ __device__ __forceinline__ uint32_t or_relaxed(uint32_t *p, uint32_t v)
 		     : "=r"(old) : "l"(p), "r"(v) : "memory");
 	return old;
 }
+__device__ __forceinline__ uint32_t cas_release(uint32_t *p, uint32_t cmp, uint32_t val)
+{
+	uint32_t old;
+	asm volatile("atom.release.gpu.global.cas.b32 %0, [%1], %2, %3;"
+		     : "=r"(old) : "l"(p), "r"(cmp), "r"(val) : "memory");
+	return old;
+}
+__device__ __forceinline__ unsigned long long add64_relaxed(unsigned long long *p, unsigned long long v)
+{
+	unsigned long long old;
+	asm volatile("atom.relaxed.gpu.global.add.u64 %0, [%1], %2;"
+		     : "=l"(old) : "l"(p), "l"(v) : "memory");
+	return old;
+}
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p)
+{
+	unsigned long long v;
+	asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v)
+{
+	asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 __device__ __forceinline__ uint32_t and_release(uint32_t *p, uint32_t v)
 {
 	uint32_t old;
@@ -398,17 +422,22 @@ __device__ __forceinline__ int64_t msq_dequeue(kma_heap *h)
  * "filled by the enqueue with ticket p", seq == p means "free for the
  * enqueue with ticket p".  ring_avail counts completed enqueues not yet
  * claimed by a dequeue; a dequeue needs two (one stays behind, as the
- * reference's dummy does). */
+ * reference's dummy does).  The ring carries only superblock numbers: the
+ * enqueuer publishes with a release store (ordering its detach of the
+ * superblock first), and everything a dequeuer then writes is addressed
+ * through the number it read, so tickets, counts and the slot read are
+ * relaxed; a count seen before its slot store only makes a dequeuer wait
+ * on the slot's sequence number. */
 __device__ __forceinline__ int ring_enqueue(kma_heap *h, uint32_t s)
 {
-	unsigned long long pos = add64_acqrel(&h->free_tail.v, 1ull);
+	unsigned long long pos = add64_relaxed(&h->free_tail.v, 1ull);
 	unsigned long long *slot = &h->ring[pos % h->ring_cap];
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
-		unsigned long long w = ld_acquire64(slot);
+		unsigned long long w = ld_relaxed64(slot);
 		if ((uint32_t)(w >> 32) == (uint32_t)pos) {
 			st_release64(slot, ((unsigned long long)(uint32_t)(pos + 1) << 32) | s);
-			add_acqrel(&h->ring_avail.v, 1u);
+			atomicAdd(&h->ring_avail.v, 1u);
 			return 1;
 		}
 		backoff(it);
@@ -424,12 +453,12 @@ __device__ __forceinline__ int64_t ring_dequeue(kma_heap *h)
 	if (old < 2) {
 		/* near empty: undo, then claim only a count that is really there */
 		atomicAdd(avail, 1);
-		int32_t a = (int32_t)ld_acquire(&h->ring_avail.v);
+		int32_t a = (int32_t)ld_relaxed(&h->ring_avail.v);
 		uint32_t lim = h->spin_limit, it = 0;
 		for (;;) {
 			if (a < 2)
 				return -1;
-			int32_t seen = (int32_t)cas_acqrel(&h->ring_avail.v, (uint32_t)a, (uint32_t)(a - 1));
+			int32_t seen = (int32_t)atomicCAS((unsigned *)&h->ring_avail.v, (uint32_t)a, (uint32_t)(a - 1));
 			if (seen == a)
 				break;
 			a = seen;
@@ -439,13 +468,13 @@ __device__ __forceinline__ int64_t ring_dequeue(kma_heap *h)
 			}
 		}
 	}
-	unsigned long long pos = add64_acqrel(&h->free_head.v, 1ull);
+	unsigned long long pos = add64_relaxed(&h->free_head.v, 1ull);
 	unsigned long long *slot = &h->ring[pos % h->ring_cap];
 	uint32_t lim = h->spin_limit;
 	for (uint32_t it = 0; it < lim; it++) {
-		unsigned long long w = ld_acquire64(slot);
+		unsigned long long w = ld_relaxed64(slot);
 		if ((uint32_t)(w >> 32) == (uint32_t)(pos + 1)) {
-			st_release64(slot, (unsigned long long)(uint32_t)(pos + h->ring_cap) << 32);
+			st_relaxed64(slot, (unsigned long long)(uint32_t)(pos + h->ring_cap) << 32);
 			return (int64_t)(uint32_t)w;
 		}
 		backoff(it);
@@ -487,7 +516,6 @@ __device__ __forceinline__ void sb_format(kma_heap *h, uint32_t s, uint32_t c, u
 		*bitmap_word(h, sb, k) = v;
 	}
 	h->sb_home[s] = (uint16_t)shard;
-	fence_acqrel();
 	st_release(&h->sb_state[s], st_make(c, slots, fr));
 }
 
@@ -571,7 +599,7 @@ __device__ inline void *kma_malloc(kma_heap *h, size_t size)
 			 * of that class then spins on a full superblock until the
 			 * block is freed (kma.cl:203-204).  Leave the class empty
 			 * instead, which is what taking the last slot does. */
-			cas_acqrel(clsw, KMA_POISON, slots == 1 ? 0u : (uint32_t)s + KMA_CLS_BASE);
+			cas_release(clsw, KMA_POISON, slots == 1 ? 0u : (uint32_t)s + KMA_CLS_BASE);
 			return sb_get_block(h, (uint32_t)s, c, slots - 1);
 		}
 		if (cur == KMA_POISON) {
@@ -778,10 +806,13 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 			/* the refiller takes the top t slots, which are exactly the
 			 * hints slots-1 .. slots-t of t serial reservations */
 			uint32_t pub = t == slots ? 0u : (uint32_t)s + KMA_CLS_BASE;
+			/* release: a thread that finds s in the slot must find
+			 * its formatted state (a stale one would read as full and
+			 * get s detached with free slots nobody can reach) */
 			if (locked)
-				cas_acqrel(clsw, KMA_POISON, pub);
+				cas_release(clsw, KMA_POISON, pub);
 			else if (pub)
-				cas_acqrel(clsw, 0, pub);
+				cas_release(clsw, 0, pub);
 			r.sb = (uint32_t)s;
 			r.cls = c;
 			r.left = t;
@@ -807,6 +838,10 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		}
 		uint32_t fr = st_free(st);
 		uint32_t t = want < fr ? want : fr;
+		/* the first bitmap word the claim will visit is known already:
+		 * load it alongside the CAS instead of after it */
+		uint32_t k0 = (fr - t) >> 5;
+		uint32_t spec = ld_relaxed(bitmap_word(h, sb_addr(h, s), k0));
 		if (cas_relaxed(stp, st, st - t) != st) {
 			tally(tl, KMA_T_CASFAIL);
 			continue;
@@ -818,7 +853,8 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		r.left = t;
 		r.cursor = fr - t; /* lowest of the t serial hints fr-1 .. fr-t */
 		r.pre = false;
-		r.kword = 0xffffffffu;
+		r.kword = k0;
+		r.known = spec;
 		r.hint = fr - 1;
 		return 1;
 	}
@@ -874,6 +910,12 @@ __device__ __forceinline__ uint32_t warp_claim_step(kma_heap *h, warp_resv &r, u
 			r.cursor = (k + 1) * 32;
 			if (r.cursor >= slots)
 				r.cursor = 0;
+			/* what is known of this word may predate the reservation
+			 * (the speculative load): the next visit, possibly of this
+			 * same word after a wrap, claims afresh.  An atomicOr's
+			 * result always shows at least `left` clear bits, which
+			 * is what guarantees progress. */
+			r.kword = 0xffffffffu;
 		}
 	}
 	return got;

@@ -172,10 +172,12 @@ def test_c2_full_size_invariants(mode, heap):
         st = wl.stats()
         assert st["bad_tags"] == 0 and st["frees"] == st["mallocs"] - st["nulls"]
         img = h.snapshot()
-        assert ins.check_canonical_empty(img, h.bitmaps()) == []
         flags = h.error_flags()
+        assert ins.check_canonical_empty(img, h.bitmaps()) == [], f"error flags {flags}"
         assert not flags & kma_b200.KMA_FLAG_BADFREE
-        if not h.compat:
+        # the warp path gives up only on a spin limit, and none is reached
+        # here; the plain path on the single-queue heap may starve a thread
+        if not h.compat or mode == MODE_WARP:
             assert flags == 0
 
 
