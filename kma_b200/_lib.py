@@ -61,7 +61,20 @@ class KmaWlStats(Structure):
                 ("verify_bytes", c_uint64)]
 
 
-# (name, restype, argtypes) for every symbol include/kma.h declares
+class KmaC3QueueStats(Structure):
+    _fields_ = [("enqueued", c_uint64), ("dequeued", c_uint64), ("empty", c_uint64),
+                ("remaining", c_uint64), ("out_count", c_uint64), ("out_xor", c_uint64),
+                ("out_sum", c_uint64), ("in_xor", c_uint64), ("in_sum", c_uint64),
+                ("err", c_uint32), ("walk_ok", c_uint32), ("enqueue_ms", c_float),
+                ("dequeue_ms", c_float)]
+
+
+class KmaC3TreeStats(Structure):
+    _fields_ = [("live_keys", c_uint64), ("keys_xor", c_uint64), ("keys_sum", c_uint64),
+                ("sorted", c_uint32), ("err", c_uint32), ("ms", c_float)]
+
+
+# (name, restype, argtypes) for every symbol include/*.h declares
 SIGNATURES = [
     ("kma_size_by_sbid", c_uint32, [c_uint32, c_int]),
     ("kma_slots_by_size", c_int, [c_uint32, c_uint64]),
@@ -98,6 +111,38 @@ SIGNATURES = [
     ("kma_wl_live", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("kma_debug_set_class_word", c_int, [c_void_p, c_uint32, c_uint32, c_void_p]),
     ("kma_bench_atomics", c_int, [c_int, c_uint64, c_uint32, c_uint32, c_void_p, POINTER(c_float)]),
+    # include/kma_structs.h
+    ("kma_pma_create", c_int, [c_uint64, c_int, c_void_p, POINTER(c_void_p)]),
+    ("kma_pma_destroy", c_int, [c_void_p]),
+    ("kma_pma_device_ptr", c_void_p, [c_void_p]),
+    ("kma_pma_base", c_void_p, [c_void_p]),
+    ("kma_pma_reset", c_int, [c_void_p, c_void_p]),
+    ("kma_pma_head", c_int, [c_void_p, c_void_p, POINTER(c_uint64)]),
+    ("kma_pma_replay_host", c_int, [c_void_p, c_void_p, c_int64, c_void_p]),
+    ("kma_clqueue_create", c_int, [c_int, c_void_p, POINTER(c_void_p)]),
+    ("kma_clqueue_destroy", c_int, [c_void_p]),
+    ("kma_clqueue_device_ptr", c_void_p, [c_void_p]),
+    ("kma_iqueue_create", c_int, [c_void_p, c_uint32, c_uint32, c_void_p, c_uint32, c_int, c_void_p,
+                                  POINTER(c_void_p)]),
+    ("kma_iqueue_destroy", c_int, [c_void_p]),
+    ("kma_iqueue_device_ptr", c_void_p, [c_void_p]),
+    ("kma_iqueue_error_flags", c_int, [c_void_p, c_void_p, POINTER(c_uint32), c_int]),
+    ("kma_cltree_create", c_int, [c_int, c_void_p, POINTER(c_void_p)]),
+    ("kma_cltree_destroy", c_int, [c_void_p]),
+    ("kma_cltree_device_ptr", c_void_p, [c_void_p]),
+    ("kma_clarraylist_create", c_int, [c_uint32, c_void_p, c_void_p, c_void_p, POINTER(c_void_p)]),
+    ("kma_clarraylist_destroy", c_int, [c_void_p]),
+    ("kma_clarraylist_device_ptr", c_void_p, [c_void_p]),
+    ("kma_clqueue_replay_host", c_int, [c_uint32, c_void_p, c_int64, c_void_p, c_void_p]),
+    ("kma_iqueue_replay_host", c_int, [c_uint32, c_uint32, c_void_p, c_int64, c_void_p, c_void_p]),
+    ("kma_cltree_replay_host", c_int, [c_void_p, c_int64, c_void_p, c_void_p, POINTER(c_int64)]),
+    ("kma_clarraylist_replay_host", c_int, [c_void_p, c_void_p, c_uint32, c_void_p, c_int64, c_void_p]),
+    ("kma_clarraylist_group_host", c_int, [c_void_p, c_void_p, c_uint32, c_void_p, c_uint32, c_int,
+                                           c_void_p]),
+    ("kma_c3_queue_run", c_int, [c_int, c_uint32, c_uint32, c_uint32, c_uint64, c_int,
+                                 POINTER(KmaC3QueueStats)]),
+    ("kma_c3_tree_run", c_int, [c_void_p, c_void_p, c_uint64, c_uint32, c_int, c_void_p,
+                                POINTER(KmaC3TreeStats)]),
 ]
 
 _lib = None

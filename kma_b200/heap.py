@@ -80,9 +80,10 @@ class Heap:
         return self._h
 
     def close(self) -> None:
-        if getattr(self, "_h", None) is not None:
-            check(lib().kma_destroy(self._h), "kma_destroy")
-            self._h = None
+        h = getattr(self, "_h", None)
+        if h is not None:
+            self._h = None  # never destroyed twice, even when destroy reports an error
+            check(lib().kma_destroy(h), "kma_destroy")
 
     def __enter__(self):
         return self
@@ -172,9 +173,10 @@ class Workload:
         self._w = w
 
     def close(self) -> None:
-        if getattr(self, "_w", None) is not None:
-            check(lib().kma_wl_destroy(self._w), "kma_wl_destroy")
+        w = getattr(self, "_w", None)
+        if w is not None:
             self._w = None
+            check(lib().kma_wl_destroy(w), "kma_wl_destroy")
 
     def __enter__(self):
         return self

@@ -68,6 +68,8 @@ void *oref_heap_create(unsigned int sblocks)
 	return raw;
 }
 void oref_heap_destroy(void *h) { free(h); }
+/* the first superblock (offsets in the replays are measured from here) */
+void *oref_heap_sb_base(void *h) { return (char *)h + sizeof(struct clheap); }
 void *oref_heap_malloc(void *h, uint64_t n) { return (void *)kma_malloc(h, (size_t)n); }
 void oref_heap_free(void *h, void *p) { kma_free(h, (uintptr_t)p); }
 
