@@ -74,6 +74,21 @@ class KmaC3TreeStats(Structure):
                 ("sorted", c_uint32), ("err", c_uint32), ("ms", c_float)]
 
 
+class KmaBatchJob(Structure):
+    _fields_ = [("threads", c_uint32), ("pad", c_uint32), ("seed", c_uint64)]
+
+
+class KmaBatchStats(Structure):
+    _fields_ = [("mallocs", c_uint64), ("frees", c_uint64), ("nulls", c_uint64), ("bad_tags", c_uint64),
+                ("fill_bytes", c_uint64), ("verify_bytes", c_uint64), ("cache_hits", c_uint64),
+                ("cache_puts", c_uint64), ("retired", c_uint64)]
+
+
+class KmaBatchTuneEntry(Structure):
+    _fields_ = [("sb_size_log2", c_uint32), ("block_dim", c_uint32), ("cache_depth", c_uint32),
+                ("pad", c_uint32), ("ms", c_float), ("mops", c_float), ("stats", KmaBatchStats)]
+
+
 # (name, restype, argtypes) for every symbol include/*.h declares
 SIGNATURES = [
     ("kma_size_by_sbid", c_uint32, [c_uint32, c_int]),
@@ -143,6 +158,17 @@ SIGNATURES = [
                                  POINTER(KmaC3QueueStats)]),
     ("kma_c3_tree_run", c_int, [c_void_p, c_void_p, c_uint64, c_uint32, c_int, c_void_p,
                                 POINTER(KmaC3TreeStats)]),
+    # include/kma_batch.h
+    ("kma_batch_create", c_int, [c_void_p, POINTER(KmaBatchJob), c_uint32, c_uint32, POINTER(c_void_p)]),
+    ("kma_batch_destroy", c_int, [c_void_p]),
+    ("kma_batch_items", c_uint64, [c_void_p]),
+    ("kma_batch_run", c_int, [c_void_p, c_uint32, c_uint32, c_void_p]),
+    ("kma_batch_capture", c_int, [c_void_p, c_uint32, c_uint32, c_void_p]),
+    ("kma_batch_launch", c_int, [c_void_p, c_void_p]),
+    ("kma_batch_stats_get", c_int, [c_void_p, c_void_p, POINTER(KmaBatchStats)]),
+    ("kma_batch_autotune", c_int, [POINTER(KmaBatchJob), c_uint32, c_uint32, c_uint64, c_void_p, c_uint32,
+                                   c_void_p, c_uint32, c_void_p, c_uint32, c_uint32, c_uint32, c_int,
+                                   POINTER(KmaBatchTuneEntry), POINTER(c_uint32)]),
 ]
 
 _lib = None
