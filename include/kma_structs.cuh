@@ -708,6 +708,19 @@ __device__ inline void *kma_clarraylist_grow_block(kma_clarraylist *l, uint32_t 
 	return reinterpret_cast<unsigned char *>(page) + before * l->obj_size;
 }
 
+/* Each calling lane grows its OWN list (l differs per lane) by `objs`
+ * objects; the page mallocs of the warp go to the heap together
+ * (kma_malloc_warp / kma_pma_malloc_warp).  Same page layout and result as
+ * kma_clarraylist_grow per lane; no counterpart in the reference. */
+__device__ inline void *kma_clarraylist_grow_lanes(kma_clarraylist *l, uint32_t objs)
+{
+	size_t size = (size_t)objs * l->obj_size + KMA_AL_PAGE_HDR;
+	void *p = kma_detail::al_heap_malloc<true>(l, size);
+	if (!p)
+		return nullptr;
+	return kma_detail::al_page_init(l, p, objs);
+}
+
 /* clArrayList_get (clArrayList.cl:178-200): object i, walking the pages in
  * growth order; NULL past the end (the reference returns an uninitialised
  * value there). */
@@ -736,6 +749,27 @@ __device__ inline void kma_clarraylist_clear(kma_clarraylist *l)
 		if (!p)
 			return;
 		al_heap_free(l, reinterpret_cast<void *>(p));
+	}
+}
+
+/* Each calling lane clears its OWN list; the warp's page frees go to the
+ * heap together (kma_free_warp).  Every lane of the warp that calls it
+ * must take part until all of their lists are empty. */
+__device__ inline void kma_clarraylist_clear_lanes(kma_clarraylist *l)
+{
+	using namespace kma_detail;
+	const uint32_t active = __activemask();
+	bool more = true;
+	while (__any_sync(active, more)) {
+		unsigned long long p = 0;
+		if (more) {
+			p = clq_dequeue<clq_link_aligned>(&l->queue, &l->err, KMA_STRUCT_SPIN);
+			more = p != 0;
+		}
+		if (l->heap_kind == KMA_AL_HEAP_PMA)
+			kma_pma_free((kma_pma *)l->heap, reinterpret_cast<void *>(p));
+		else
+			kma_free_warp((kma_heap *)l->heap, reinterpret_cast<void *>(p));
 	}
 }
 

@@ -7,7 +7,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import (POINTER, Structure, c_char_p, c_float, c_int, c_int32, c_int64, c_uint,
+from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_uint,
                     c_uint32, c_uint64, c_void_p)
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -87,6 +87,26 @@ class KmaBatchStats(Structure):
 class KmaBatchTuneEntry(Structure):
     _fields_ = [("sb_size_log2", c_uint32), ("block_dim", c_uint32), ("cache_depth", c_uint32),
                 ("pad", c_uint32), ("ms", c_float), ("mops", c_float), ("stats", KmaBatchStats)]
+
+
+class KmaServeCfg(Structure):
+    _fields_ = [("slots", c_uint32), ("max_vertices", c_uint32), ("deg_max", c_uint32),
+                ("block_dim", c_uint32), ("gamma", c_float), ("occupancy_limit", c_float)]
+
+
+class KmaServeReq(Structure):
+    _fields_ = [("n_vertices", c_uint32), ("pad", c_uint32), ("seed", c_uint64), ("arrival_s", c_double)]
+
+
+class KmaServeResult(Structure):
+    _fields_ = [("checksum", c_uint64), ("edges", c_uint64), ("mallocs", c_uint64), ("frees", c_uint64),
+                ("nulls", c_uint64), ("admit_s", c_double), ("done_s", c_double),
+                ("reserved_bytes", c_uint64), ("slot", c_uint32), ("status", c_uint32)]
+
+
+class KmaServeSummary(Structure):
+    _fields_ = [("wall_s", c_double), ("ops", c_uint64), ("max_running", c_uint32),
+                ("max_sb_in_use", c_uint32), ("max_occupancy", c_double)]
 
 
 # (name, restype, argtypes) for every symbol include/*.h declares
@@ -169,6 +189,12 @@ SIGNATURES = [
     ("kma_batch_autotune", c_int, [POINTER(KmaBatchJob), c_uint32, c_uint32, c_uint64, c_void_p, c_uint32,
                                    c_void_p, c_uint32, c_void_p, c_uint32, c_uint32, c_uint32, c_int,
                                    POINTER(KmaBatchTuneEntry), POINTER(c_uint32)]),
+    # include/kma_serve.h
+    ("kma_serve_create", c_int, [c_void_p, POINTER(KmaServeCfg), POINTER(c_void_p)]),
+    ("kma_serve_destroy", c_int, [c_void_p]),
+    ("kma_serve_estimate", c_uint64, [c_void_p, c_uint32]),
+    ("kma_serve_run", c_int, [c_void_p, POINTER(KmaServeReq), c_uint32, c_int, POINTER(KmaServeResult),
+                              POINTER(KmaServeSummary)]),
 ]
 
 _lib = None
