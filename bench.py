@@ -15,8 +15,10 @@ between steps, outside the timed events), max over ranks; N > 1 runs
 independent per-GPU heap replicas (weak scaling: the heap does not shard
 and has no exchange step).  It also reports the plain per-thread kernel on
 the same GPU, the roofline of the dominant kernel, the CPU baseline, the
-end-to-end figure through the host-buffer C ABI call, and the invariant
-check of one extra step.  The reference arm times the reference's own
+end-to-end figure through the host-buffer C ABI call, the invariant check
+of one extra step, and (under "forms") the other configurations: the
+lock-free structures (config 3), the autotuned batched form (config 4) and
+the served form's p50/p99 latency at swept arrival rates (config 5).  The reference arm times the reference's own
 kma.cl built as host C (oracle/_ref) on the host cores.
 """
 from __future__ import annotations
@@ -171,6 +173,99 @@ def run_reference(args) -> int:
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+# ------------------------------------------------------ other forms (rank 0)
+def tree_expected(kinds, keys):
+    """Sequential results of the config-3 tree ops (1 inserted / 0 exists /
+    2 revived; lookup 1 found / 0; remove 1 / 0): keys seen once are decided
+    in bulk, repeated keys replayed in op order."""
+    import numpy as np
+    res = np.where(kinds == 0, 1, 0).astype(np.int8)
+    uniq, inv, cnt = np.unique(keys, return_inverse=True, return_counts=True)
+    rep = np.nonzero(cnt[inv] > 1)[0]
+    live, seen = {}, set()
+    for j in rep:
+        k, kind = int(keys[j]), int(kinds[j])
+        if kind == 0:
+            res[j] = 1 if k not in seen else (0 if live[k] else 2)
+            seen.add(k)
+            live[k] = True
+        elif kind == 1:
+            res[j] = 1 if live.get(k, False) else 0
+        else:
+            res[j] = 1 if live.get(k, False) else 0
+            if k in live:
+                live[k] = False
+    n_live = int(np.sum((cnt[inv] == 1) & (kinds == 0))) + sum(1 for v in live.values() if v)
+    return res, n_live
+
+
+def measure_forms(quick: bool = False) -> dict:
+    """Config 3 (structures), 4 (batched, autotuned) and 5 (served) on this
+    GPU: each its own workload at its configured size, timed on the device."""
+    import numpy as np
+    from kma_b200 import Heap, structs
+    from kma_b200.batch import autotune, c4_jobs
+    from kma_b200.serve import Server, c5_requests
+    out = {}
+    # config 3: 2^24 payloads by 2^18 threads x 64; tree 2^22 ops 50/30/20
+    c3 = {}
+    for name, kind in (("clqueue", structs.C3_CLQUEUE), ("iqueue", structs.C3_IQUEUE)):
+        for shards, thr, per in ((4096, 1 << 18, 64), (1, 1 << 12, 16)):
+            st = structs.c3_queue(kind, thr, per, shards, seed=0xC3)
+            n = thr * per
+            ok = (st["out_count"] == n and st["out_xor"] == st["in_xor"] and st["out_sum"] == st["in_sum"]
+                  and st["walk_ok"] == 1 and st["err"] == 0)
+            c3[f"{name}_shards{shards}"] = {
+                "payloads": n, "threads": thr, "conserved": bool(ok),
+                "enqueue_mops": round(n / st["enqueue_ms"] / 1e3, 1),
+                "dequeue_mops": round(n / st["dequeue_ms"] / 1e3, 1)}
+    rng = np.random.default_rng(0xC3)
+    nt = 1 << 22
+    kinds = rng.choice(3, size=nt, p=(0.5, 0.3, 0.2)).astype(np.uint8)
+    keys = rng.integers(0, 1 << 32, size=nt, dtype=np.uint64).astype(np.uint32)
+    res, st = structs.c3_tree(kinds, keys, threads=1 << 18)
+    exp, n_live = tree_expected(kinds, keys)
+    c3["tree"] = {"ops": nt, "mops": round(nt / st["ms"] / 1e3, 1),
+                  "equals_sequential": bool(np.array_equal(res, exp) and st["live_keys"] == n_live
+                                            and st["sorted"] == 1 and st["err"] == 0)}
+    out["structures_c3"] = c3
+    # config 4: 64 jobs of 1k..1M threads, 16 GiB heap, autotuned
+    t, sd = c4_jobs()
+    grid = dict(sb_log2s=(12, 14, 16), block_dims=(128, 256, 512), depths=(0, 2, 4)) if not quick else \
+        dict(sb_log2s=(12,), block_dims=(256,), depths=(0, 4))
+    entries, best = autotune(t, sd, rounds=16, heap_bytes=16 << 30, warmup=1, reps=2, **grid)
+    b = entries[best]
+    out["batched_c4"] = {
+        "jobs": 64, "work_items": int(t.sum()), "rounds": 16, "heap_bytes": 16 << 30,
+        "best": {"sb_size": b["sb_size"], "block_dim": b["block_dim"], "cache_depth": b["cache_depth"],
+                 "mops": b["mops"], "ms_per_launch": b["ms"],
+                 "null_frac": round(b["nulls"] / b["mallocs"], 4), "bad_tags": b["bad_tags"]},
+        "grid": [[e["sb_size"], e["block_dim"], e["cache_depth"], e["mops"],
+                  round(e["nulls"] / e["mallocs"], 4)] for e in entries],
+        "grid_cols": ["sb_size", "block_dim", "cache_depth", "mops", "null_frac"],
+        "launch": "one CUDA graph per configuration: heap reset + job seeding + one persistent kernel"}
+    # config 5: 64 GiB resident heap, Poisson arrivals at swept rates
+    served = []
+    with Heap((64 << 30) >> 14, 14) as h, Server(h, slots=16) as srv:
+        for rate in ((200, 3200, 0) if not quick else (3200,)):
+            nv, seeds, arr = c5_requests(0xC5, 300, rate=rate if rate else 1.0)
+            res_s, summ = srv.run(nv, seeds, arr if rate else None, realtime=bool(rate))
+            lat = np.array([r["latency_s"] for r in res_s if r["status"] == "ok"])
+            served.append({"rate_per_s": rate or "all at once", "requests": len(res_s),
+                           "ok": int(sum(r["status"] == "ok" for r in res_s)),
+                           "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+                           "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
+                           "mops": round(summ["ops"] / summ["wall_s"] / 1e6, 1),
+                           "requests_per_s": round(len(res_s) / summ["wall_s"], 1),
+                           "max_running": summ["max_running"],
+                           "max_occupancy": round(summ["max_occupancy"], 4)})
+        flags = h.error_flags()
+    out["served_c5"] = {"heap_bytes": 64 << 30, "slots": 16, "occupancy_limit": 0.85,
+                        "graph": "N log-uniform 1k..4M vertices, degrees ~ d^-2.1 on 1..4096",
+                        "heap_error_flags": flags, "loads": served}
+    return out
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -380,6 +475,8 @@ def run_ours(args) -> int:
                                   "peak = returning atomicAdd on distinct 128-B lines, all SMs"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 4 * args.steps, "clocks": clocks,
         }
+        if not args.no_forms:
+            out["forms"] = measure_forms()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -405,6 +502,8 @@ def main(argv=None) -> int:
     ap.add_argument("--sblocks", type=int, default=SBLOCKS, help="superblocks in the heap")
     ap.add_argument("--sb-log2", type=int, default=SB_LOG2, help="superblock size (experiments)")
     ap.add_argument("--shards", type=int, default=0, help="most class-table shards per class")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the structure, batched and served measurements")
     ap.add_argument("--only-timed", action="store_true",
                     help="run the timed steps only and print a short line (profiling)")
     args = ap.parse_args(argv)
