@@ -651,6 +651,19 @@ __device__ __forceinline__ void sb_recycle(kma_heap *h, uint32_t s, uint32_t c)
 }
 } /* namespace kma_detail */
 
+/* The start of the heap block that contains p (p may point inside it), or
+ * NULL when p is not inside a superblock in use.  For structures that
+ * place an aligned object inside a 4-byte aligned block and must free the
+ * block itself.  No counterpart in the reference. */
+__device__ __forceinline__ void *kma_block_of(kma_heap *h, const void *p)
+{
+	using namespace kma_detail;
+	uint32_t s, c, slot;
+	if (!p || !block_locate(h, p, s, c, slot))
+		return NULL;
+	return sb_addr(h, s) + KMA_SB_HDR + (size_t)slot * h->cls_size[c];
+}
+
 /* kma.cl:305-373 */
 __device__ inline void kma_free(kma_heap *h, void *p)
 {

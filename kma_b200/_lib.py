@@ -109,6 +109,12 @@ class KmaServeSummary(Structure):
                 ("max_sb_in_use", c_uint32), ("max_occupancy", c_double)]
 
 
+class KmaGraphStats(Structure):
+    _fields_ = [("nodes", c_uint64), ("links", c_uint64), ("lost_adds", c_uint64), ("nulls", c_uint64),
+                ("edge_xor", c_uint64), ("edge_sum", c_uint64), ("sorted", c_uint32), ("err", c_uint32),
+                ("build_ms", c_float), ("pad", c_float)]
+
+
 # (name, restype, argtypes) for every symbol include/*.h declares
 SIGNATURES = [
     ("kma_size_by_sbid", c_uint32, [c_uint32, c_int]),
@@ -189,6 +195,10 @@ SIGNATURES = [
     ("kma_batch_autotune", c_int, [POINTER(KmaBatchJob), c_uint32, c_uint32, c_uint64, c_void_p, c_uint32,
                                    c_void_p, c_uint32, c_void_p, c_uint32, c_uint32, c_uint32, c_int,
                                    POINTER(KmaBatchTuneEntry), POINTER(c_uint32)]),
+    # include/kma_graph.h
+    ("kma_graph_edge_mix", c_uint64, [c_uint32, c_uint32]),
+    ("kma_graph_build", c_int, [c_void_p, c_void_p, c_uint64, c_uint32, c_int, POINTER(KmaGraphStats),
+                                c_void_p, c_void_p, c_void_p, c_void_p]),
     # include/kma_serve.h
     ("kma_serve_create", c_int, [c_void_p, POINTER(KmaServeCfg), POINTER(c_void_p)]),
     ("kma_serve_destroy", c_int, [c_void_p]),

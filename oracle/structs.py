@@ -55,6 +55,8 @@ def _cl_lib() -> ctypes.CDLL:
             ("oref_al_grow", c_uint64, [c_void_p, c_uint32]), ("oref_al_get", c_uint64, [c_void_p, c_uint64]),
             ("oref_al_clear", None, [c_void_p]),
             ("oref_al_grow_local_group", c_int, [c_void_p, c_uint32, c_void_p, c_void_p]),
+            ("oref_graph_node_size", c_uint32, []), ("oref_graph_link_size", c_uint32, []),
+            ("oref_graph_build_serial", None, [c_void_p, c_void_p, c_void_p, c_uint32]),
         ]:
             f = getattr(L, name)
             f.restype = res
@@ -230,3 +232,41 @@ def pma_replay(nbytes: int, ops: np.ndarray):
     finally:
         L.oref_pma_destroy(p)
     return out
+
+
+def graph_build(sblocks: int, edges: np.ndarray):
+    """tb_clTree.cl clTree_test run by one work-item over a fresh reference
+    KMA heap of `sblocks` 4 KiB superblocks: (keys, node offsets from the
+    first superblock, link sinks, link start) with nodes in key order and
+    each node's links in queue order."""
+    L = _cl_lib()
+    assert L.oref_graph_node_size() == 40 and L.oref_graph_link_size() == 16
+    edges = np.ascontiguousarray(edges, np.uint32).reshape(-1, 2)
+    h = L.oref_heap_create(sblocks)
+    base = L.oref_heap_sb_base(h)
+    t = L.oref_tree_create()
+    u64 = lambda a: ctypes.c_uint64.from_address(a).value  # noqa: E731
+    u32 = lambda a: ctypes.c_uint32.from_address(a).value  # noqa: E731
+    try:
+        L.oref_graph_build_serial(h, t, edges.ctypes.data, len(edges))
+        keys, offs, sinks, start = [], [], [], []
+        stack, cur = [], u64(t)
+        while cur or stack:  # clGraph_node = {clTree_node (key, left, right), clqueue links}
+            while cur:
+                stack.append(cur)
+                cur = u64(cur + 8)
+            cur = stack.pop()
+            keys.append(u32(cur))
+            offs.append(cur - base)
+            start.append(len(sinks))
+            link = u64(cur + 24)  # links.head; clGraph_link = {next, sink}
+            while link:
+                sinks.append(u32(u64(link + 8)))
+                link = u64(link)
+            cur = u64(cur + 16)
+        start.append(len(sinks))
+    finally:
+        L.oref_tree_destroy(t)
+        L.oref_heap_destroy(h)
+    return (np.array(keys, np.int64), np.array(offs, np.int64), np.array(sinks, np.int64),
+            np.array(start, np.int64))

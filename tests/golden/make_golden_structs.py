@@ -8,7 +8,9 @@ the fixture is committed and the GPU tests only read it):
     python tests/golden/make_golden_structs.py
 
 Each case stores its op stream and the reference's results (and, for the
-queues, the final head/tail/links; for the tree, the in-order keys).
+queues, the final head/tail/links; for the tree, the in-order keys; for
+the graph build of test/tb_clTree.cl, every node's key, block offset and
+links in queue order).
 """
 from __future__ import annotations
 
@@ -34,6 +36,18 @@ AL_GROUP = [(41, 64, 4, [1, 2, 1, 2, 3, 0, 5, 1]), (42, 64, 8, list(range(33))),
             (43, 64, 4, [2] * 64), (44, 64, 12, [0, 0, 7, 0, 1])]  # (seed, sblocks, objsize, objs)
 PMA = [(51, 4096, 300), (52, 100000, 2000)]                  # (seed, bytes, ops)
 PMA_EDGE = [4096, 1000]
+GRAPH = [(61, 64, 400, 60), (62, 256, 3000, 700)]          # (seed, sblocks, edges, vertices)
+
+
+def graph_edges(seed: int, n_edges: int, n_vertices: int) -> np.ndarray:
+    """Synthetic edges (the reference's edge file is not shipped): Zipf(1.1)
+    vertex ranks mapped to distinct random u32 keys."""
+    rng = np.random.default_rng(seed)
+    keys = rng.choice(2**32 - 1, size=n_vertices, replace=False).astype(np.uint32)
+    p = np.arange(1, n_vertices + 1, dtype=np.float64) ** -1.1
+    p /= p.sum()
+    return np.stack([keys[rng.choice(n_vertices, size=n_edges, p=p)],
+                     keys[rng.choice(n_vertices, size=n_edges, p=p)]], axis=1).astype(np.uint32)
 
 
 def cases() -> dict:
@@ -69,6 +83,12 @@ def cases() -> dict:
         ops = ss.pma_edge_stream(nb)
         out[f"pmaedge_{nb}_ops"], out[f"pmaedge_{nb}_out"] = ops, structs.pma_replay(nb, ops)
         out[f"pmaedge_{nb}_bytes"] = np.array([nb])
+    for seed, sblocks, ne, nv in GRAPH:
+        e = graph_edges(seed, ne, nv)
+        k, o, sk, st = structs.graph_build(sblocks, e)
+        out[f"graph_{seed}_edges"], out[f"graph_{seed}_keys"] = e.astype(np.int64), k
+        out[f"graph_{seed}_offs"], out[f"graph_{seed}_sinks"], out[f"graph_{seed}_start"] = o, sk, st
+        out[f"graph_{seed}_cfg"] = np.array([sblocks])
     return out
 
 
