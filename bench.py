@@ -283,7 +283,14 @@ def run_ours(args) -> int:
 
     mode = MODE_WARP if args.mode == "warp" else MODE_PLAIN
     stream = torch.cuda.current_stream()
-    heap = Heap(SBLOCKS, SB_LOG2, stream=stream, compat=(mode == MODE_PLAIN), shards=args.shards)
+    # the warp heap's waits are bounded at 2^18 iterations (well under a
+    # second; legitimate waits here last microseconds), so a wait that
+    # cannot be met shows as a flagged NULL in its step instead of a long
+    # stall; the per-thread heap on the reference's single structures keeps
+    # the default 2^22, its threads legitimately wait far longer
+    SPIN = 0 if mode == MODE_PLAIN else 1 << 18
+    heap = Heap(SBLOCKS, SB_LOG2, stream=stream, compat=(mode == MODE_PLAIN), shards=args.shards,
+                spin_limit=SPIN)
     wl = Workload(heap, WL_C2, ITEMS)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -309,12 +316,15 @@ def run_ours(args) -> int:
             torch.distributed.barrier()
         torch.cuda.synchronize()
         evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
+        flags = torch.zeros(steps, dtype=torch.int32).pin_memory()
         if sampler:
             sampler.start()
         for k in range(steps):
             flush.zero_()  # > L2, outside the timed events
             step(hp, w, m, evs[k])
+            hp.error_flags_async(flags.data_ptr() + 4 * k, stream)  # after the step's events
         torch.cuda.synchronize()
+        timed.step_flags = [int(f) & 0xffffffff for f in flags.tolist()]
         clocks = sampler.stop() if sampler else None
         if world > 1:
             torch.distributed.barrier()
@@ -327,6 +337,7 @@ def run_ours(args) -> int:
                            else local)
     step_ms, rounds_ms, clocks = timed(heap, wl, mode, args.steps, args.warmup,
                                        None if args.only_timed else sampler)
+    step_flags = list(timed.step_flags)
     st = wl.stats(stream)
     if args.only_timed:
         if rank == 0:
@@ -452,6 +463,9 @@ def run_ours(args) -> int:
             "config": {"workload": WORKLOAD, "mode": args.mode, "items": ITEMS, "rounds": ROUNDS,
                        "heap_bytes": SBLOCKS << SB_LOG2, "sb_size": 1 << SB_LOG2,
                        "ops_per_step": ops_step, "nulls": int(st["nulls"]),
+                       "step_ms_min": round(min(step_ms), 3), "step_ms_max": round(max(step_ms), 3),
+                       "step_error_flags": sorted({f for f in step_flags if f}),
+                       "spin_limit": SPIN or (1 << 22),
                        "invariant_faults": faults, "heap_error_flags": flags,
                        "l2": "inputs larger than L2 (1 GiB heap) and a 256 MiB write between "
                              "steps, outside the timed events",

@@ -37,6 +37,9 @@ extern "C" {
 /* heap error flags (kma_error_flags) */
 #define KMA_FLAG_TIMEOUT 1u  /* a bounded device spin expired */
 #define KMA_FLAG_BADFREE 2u  /* free of a pointer that is not a live block */
+/* bits 8..16 name the wait that set KMA_FLAG_TIMEOUT (KMA_ERR_AT_* in
+ * kma_device.cuh): MS queue, ring enqueue, ring count, ring dequeue, plain
+ * claim, plain reservation, plain free, warp reservation, warp turns */
 
 /* allocation modes of the workload / replay kernels */
 #define KMA_MODE_PLAIN 0     /* per-thread kma_malloc / kma_free */
@@ -56,11 +59,10 @@ typedef struct kma_config {
 	uint32_t sb_size_log2; /* 12..16: 4 KiB (the reference's KMA_SB_SIZE, kma.h:27) .. 64 KiB */
 	uint32_t spin_limit;   /* bound on every device spin; 0 = default (1<<22) */
 	int32_t device;        /* CUDA ordinal; -1 = current device */
-	uint32_t shards;       /* most class-table shards per class (1..1024); a warp uses
+	uint32_t shards;       /* most class-table shards per class (1..2048); a warp uses
 				* shard (global warp id) % shards(class).  Each class gets
-				* max((sblocks-1)/64, (sblocks-1)/32/slots(class)) shards,
-				* clamped to [1, shards]; 0 = 1024.  COMPAT forces 1 (the
-				* reference's single table) */
+				* (sblocks-1)/32 shards clamped to [1, shards]; 0 = 2048.
+				* COMPAT forces 1 (the reference's single table) */
 	uint32_t flags;        /* KMA_CFG_* */
 } kma_config;
 
@@ -104,6 +106,11 @@ int kma_get_info(kma_heap_t h, kma_info *out);
 /* Sticky device error flags (KMA_FLAG_*); clear != 0 resets them.
  * Synchronises the stream. */
 int kma_error_flags(kma_heap_t h, void *stream, uint32_t *flags, int clear);
+/* Stream-ordered copy of the error flags into *dst (device or pinned host
+ * memory), without waiting: lets a caller record the flags of each of
+ * several queued runs (a reset clears them).  No counterpart in the
+ * reference. */
+int kma_error_flags_async(kma_heap_t h, void *stream, uint32_t *dst);
 const char *kma_strerror(int err);
 /* Library build id string. */
 const char *kma_version(void);

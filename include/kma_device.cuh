@@ -28,12 +28,11 @@
  * that shard's current superblock for class c), every one on its own
  * 128-byte line.  A warp uses shard (global warp id) % cls_nsh[c], so one
  * thread of warp 0 -- a serial replay -- always uses shard 0; a heap with
- * one shard per class is the reference's single table.  Only a
- * superblock's current slots are contended, and a class with few slots per
- * superblock refills that many times more often, so kma_create gives each
- * class shards in inverse proportion to its slots (the few-slot classes get
- * the most parallel refill streams) within a budget of pinned current
- * superblocks proportional to the heap.
+ * one shard per class is the reference's single table.  Only a shard's
+ * current superblock is contended, so kma_create gives every class
+ * pages/32 shards (at most 2048): enough to spread a full GPU's warps,
+ * few enough that the superblocks pinned as shards' current ones leave
+ * the heap room.
  *
  * Superblock free list, FIFO with the reference's order and its rule that
  * one superblock always stays behind as the queue's dummy
@@ -61,8 +60,8 @@
 #include <stddef.h>
 
 #define KMA_MAX_CLASSES 16
-#define KMA_MAX_SHARDS 1024    /* per class */
-#define KMA_MAX_CLS_LINES 16384 /* sum over classes */
+#define KMA_MAX_SHARDS 2048    /* per class */
+#define KMA_MAX_CLS_LINES 32768 /* sum over classes */
 #define KMA_SB_HDR 12u
 #define KMA_POISON 1u
 #define KMA_CLS_BASE 2u
@@ -80,6 +79,16 @@
 /* heap->err bits */
 #define KMA_ERR_TIMEOUT 1u
 #define KMA_ERR_BADFREE 2u
+/* with KMA_ERR_TIMEOUT: which bounded wait expired */
+#define KMA_ERR_AT_MSQ (1u << 8)        /* MS-queue free list */
+#define KMA_ERR_AT_RING_ENQ (1u << 9)   /* ring: slot not yet released */
+#define KMA_ERR_AT_RING_AVAIL (1u << 10)/* ring: availability count */
+#define KMA_ERR_AT_RING_DEQ (1u << 11)  /* ring: slot not yet filled */
+#define KMA_ERR_AT_CLAIM (1u << 12)     /* plain malloc: bitmap claim */
+#define KMA_ERR_AT_MALLOC (1u << 13)    /* plain malloc: reservation */
+#define KMA_ERR_AT_FREE (1u << 14)      /* plain free: count update */
+#define KMA_ERR_AT_RESERVE (1u << 15)   /* warp malloc: reservation (POISON / stale waits) */
+#define KMA_ERR_AT_WARP (1u << 16)      /* warp malloc: leader turns */
 
 struct __align__(128) kma_line32 {
 	uint32_t v;
@@ -390,7 +399,7 @@ __device__ __forceinline__ int msq_enqueue(kma_heap *h, uint32_t s)
 		}
 		backoff(it);
 	}
-	set_err(h, KMA_ERR_TIMEOUT);
+	set_err(h, KMA_ERR_TIMEOUT | KMA_ERR_AT_MSQ);
 	return 0;
 }
 
@@ -414,7 +423,7 @@ __device__ __forceinline__ int64_t msq_dequeue(kma_heap *h)
 		}
 		backoff(it);
 	}
-	set_err(h, KMA_ERR_TIMEOUT);
+	set_err(h, KMA_ERR_TIMEOUT | KMA_ERR_AT_MSQ);
 	return -2;
 }
 
@@ -442,7 +451,7 @@ __device__ __forceinline__ int ring_enqueue(kma_heap *h, uint32_t s)
 		}
 		backoff(it);
 	}
-	set_err(h, KMA_ERR_TIMEOUT);
+	set_err(h, KMA_ERR_TIMEOUT | KMA_ERR_AT_RING_ENQ);
 	return 0;
 }
 
@@ -463,7 +472,7 @@ __device__ __forceinline__ int64_t ring_dequeue(kma_heap *h)
 				break;
 			a = seen;
 			if (++it >= lim) {
-				set_err(h, KMA_ERR_TIMEOUT);
+				set_err(h, KMA_ERR_TIMEOUT | KMA_ERR_AT_RING_AVAIL);
 				return -2;
 			}
 		}
@@ -479,7 +488,7 @@ __device__ __forceinline__ int64_t ring_dequeue(kma_heap *h)
 		}
 		backoff(it);
 	}
-	set_err(h, KMA_ERR_TIMEOUT);
+	set_err(h, KMA_ERR_TIMEOUT | KMA_ERR_AT_RING_DEQ);
 	return -2;
 }
 
@@ -566,7 +575,7 @@ __device__ __forceinline__ void *sb_get_block(kma_heap *h, uint32_t s, uint32_t 
 		if (slot >= slots)
 			slot = 0;
 	}
-	set_err(h, KMA_ERR_TIMEOUT);
+	set_err(h, KMA_ERR_TIMEOUT | KMA_ERR_AT_CLAIM);
 	return NULL;
 }
 
@@ -619,7 +628,7 @@ __device__ inline void *kma_malloc(kma_heap *h, size_t size)
 			cas_relaxed(clsw, cur, 0); /* kma.cl:216-218 */
 		return sb_get_block(h, s, c, fr);
 	}
-	set_err(h, KMA_ERR_TIMEOUT);
+	set_err(h, KMA_ERR_TIMEOUT | KMA_ERR_AT_MALLOC);
 	return NULL;
 }
 
@@ -709,7 +718,7 @@ __device__ inline void kma_free(kma_heap *h, void *p)
 			return;
 		}
 	}
-	set_err(h, KMA_ERR_TIMEOUT);
+	set_err(h, KMA_ERR_TIMEOUT | KMA_ERR_AT_FREE);
 }
 
 /* ------------------------------------------------------------------ */
@@ -871,7 +880,7 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		r.hint = fr - 1;
 		return 1;
 	}
-	set_err(h, KMA_ERR_TIMEOUT);
+	set_err(h, KMA_ERR_TIMEOUT | KMA_ERR_AT_RESERVE);
 	return 0;
 }
 
@@ -963,7 +972,7 @@ __device__ inline void *kma_malloc_warp(kma_heap *h, size_t size, kma_tally *tl 
 		if (++rounds > lim) {
 			if (need) {
 				need = false;
-				set_err(h, KMA_ERR_TIMEOUT);
+				set_err(h, KMA_ERR_TIMEOUT | KMA_ERR_AT_WARP);
 			}
 			continue;
 		}

@@ -127,6 +127,7 @@ SIGNATURES = [
     ("kma_heap_device_ptr", c_void_p, [c_void_p]),
     ("kma_get_info", c_int, [c_void_p, POINTER(KmaInfo)]),
     ("kma_error_flags", c_int, [c_void_p, c_void_p, POINTER(c_uint32), c_int]),
+    ("kma_error_flags_async", c_int, [c_void_p, c_void_p, c_void_p]),
     ("kma_strerror", c_char_p, [c_int]),
     ("kma_version", c_char_p, []),
     ("kma_snapshot", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,

@@ -241,26 +241,21 @@ extern "C" int kma_create_ex(const kma_config *cfg, void *stream, kma_heap_t *ou
 	 * header, i.e. sblocks - 1 superblocks enter the free list */
 	k->hh.pages = (uint32_t)nsb - 1;
 	const bool compat = cfg->flags & KMA_CFG_COMPAT;
-	/* shards per class.  Two pressures: every reservation of a class CASes
-	 * its shard's current superblock state, so each class needs enough
-	 * shards to spread the warps (a base of pages/64, measured on the
-	 * config-2 workload: ceilings of 64/256/512/1024 shards gave
-	 * 1.15/2.60/2.80/2.94 G ops/s with no NULL returns); and a
-	 * class with few slots per superblock refills that many times more
-	 * often, so it gets pages/32/slots shards if that is more.  At most
-	 * cfg->shards (default KMA_MAX_SHARDS) per class; pinned current
-	 * superblocks stay within a few percent of the heap. */
+	/* shards per class.  Every reservation of a class CASes its shard's
+	 * current superblock state, so each class needs enough shards to
+	 * spread the warps: a base of pages/32, capped at cfg->shards
+	 * (default KMA_MAX_SHARDS).  Measured on the config-2 workload (65535
+	 * pages, 9 classes in use): caps of 1024 / 2048 / 4096 gave 3.87 /
+	 * 4.11 / 4.02 G ops/s, the last with NULL returns (too many
+	 * superblocks pinned as shards' current ones); 2048 also cut the
+	 * claims that find their bits taken from 25% to 9%. */
 	uint32_t cap = compat ? 1u : (cfg->shards ? cfg->shards : KMA_MAX_SHARDS);
-	uint32_t budget = k->hh.pages / 32;
-	uint32_t base_sh = k->hh.pages / 64;
+	uint32_t base_sh = k->hh.pages / 32;
 	uint32_t lines = 0;
 	for (uint32_t c = 0; c < KMA_MAX_CLASSES; c++) {
 		uint32_t n = 0;
-		if (c < k->hh.nclasses) {
-			n = budget / k->hh.cls_slots[c];
-			n = n < base_sh ? base_sh : n;
-			n = n < 1 ? 1 : n > cap ? cap : n;
-		}
+		if (c < k->hh.nclasses)
+			n = base_sh < 1 ? 1 : base_sh > cap ? cap : base_sh;
 		k->hh.cls_nsh[c] = n;
 		k->hh.cls_base[c] = lines;
 		lines += n;
@@ -386,6 +381,15 @@ extern "C" int kma_error_flags(kma_heap_t h, void *stream, uint32_t *flags, int 
 	if (clear)
 		KMA_CUDA(cudaMemsetAsync(&h->dh->err.v, 0, 4, st));
 	KMA_CUDA(cudaStreamSynchronize(st));
+	return KMA_OK;
+}
+
+extern "C" int kma_error_flags_async(kma_heap_t h, void *stream, uint32_t *dst)
+{
+	if (!h || !dst)
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	KMA_CUDA(cudaMemcpyAsync(dst, &h->dh->err.v, 4, cudaMemcpyDefault, kma_stream(stream)));
 	return KMA_OK;
 }
 

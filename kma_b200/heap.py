@@ -112,6 +112,10 @@ class Heap:
               "kma_error_flags")
         return int(f.value)
 
+    def error_flags_async(self, dst_ptr: int, stream=None) -> None:
+        """Stream-ordered copy of the flags to dst_ptr (pinned host or device)."""
+        check(lib().kma_error_flags_async(self.handle, _stream_ptr(stream), dst_ptr), "kma_error_flags_async")
+
     def debug_set_class_word(self, cls: int, value: int, stream=None) -> None:
         """Fault injection for tests: write a raw class-table word."""
         check(lib().kma_debug_set_class_word(self.handle, cls, value, _stream_ptr(stream)),
