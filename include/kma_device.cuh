@@ -775,7 +775,7 @@ struct warp_resv {
  * number reserved, cursor = first slot to scan from, hint) and returns 1;
  * returns 0 when the heap is exhausted or a spin expired. */
 __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t want, warp_resv &r,
-		kma_tally *tl)
+		kma_tally *tl, uint32_t *hint)
 {
 	uint32_t slots = h->cls_slots[c];
 	uint32_t shard = my_shard(h, c);
@@ -799,9 +799,14 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 	}
 	uint32_t *clsw = cls_word(h, c, shard);
 	uint32_t lim = h->spin_limit;
+	/* the superblock this warp last reserved from in class c: its state is
+	 * loaded together with the class word, and used when the class word
+	 * still names it (saving the dependent load) */
+	uint32_t guess = hint ? hint[c] : 0u;
 	for (uint32_t it = 0; it < lim; it++) {
 		tally(tl, KMA_T_TRY);
 		uint32_t cur = ld_relaxed(clsw);
+		uint32_t st_guess = guess ? ld_relaxed(&h->sb_state[guess - KMA_CLS_BASE]) : 0u;
 		const bool poisoned = cur == KMA_POISON;
 		if (cur == 0 || (poisoned && slots <= KMA_PRIVATE_REFILL_SLOTS)) {
 			/* cur == 0: the reference's refill under POISON (kma.cl:166-195).
@@ -835,6 +840,8 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 				cas_release(clsw, KMA_POISON, pub);
 			else if (pub)
 				cas_release(clsw, 0, pub);
+			if (hint && pub)
+				hint[c] = pub;
 			r.sb = (uint32_t)s;
 			r.cls = c;
 			r.left = t;
@@ -852,7 +859,8 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		}
 		uint32_t s = cur - KMA_CLS_BASE;
 		uint32_t *stp = &h->sb_state[s];
-		uint32_t st = ld_relaxed(stp);
+		uint32_t st = cur == guess ? st_guess : ld_relaxed(stp);
+		guess = cur;
 		if (st_class(st) != c || st_free(st) == 0) {
 			tally(tl, KMA_T_STALE);
 			backoff(it);
@@ -870,6 +878,8 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		}
 		if (fr == t)
 			cas_relaxed(clsw, cur, 0);
+		if (hint)
+			hint[c] = cur;
 		r.sb = s;
 		r.cls = c;
 		r.left = t;
@@ -945,7 +955,13 @@ __device__ __forceinline__ uint32_t warp_claim_step(kma_heap *h, warp_resv &r, u
 
 } /* namespace kma_detail */
 
-__device__ inline void *kma_malloc_warp(kma_heap *h, size_t size, kma_tally *tl = nullptr)
+/* hint (optional): this warp's KMA_MAX_CLASSES words, zeroed once, best
+ * in shared memory; the warp's leaders remember there, per class, the
+ * superblock they last reserved from, and load its state together with
+ * the class word on the next call.  Only a speed hint: any content is
+ * safe, a stale one costs the dependent load it would have saved. */
+__device__ inline void *kma_malloc_warp(kma_heap *h, size_t size, kma_tally *tl = nullptr,
+		uint32_t *hint = nullptr)
 {
 	using namespace kma_detail;
 	const uint32_t active = __activemask();
@@ -980,7 +996,7 @@ __device__ inline void *kma_malloc_warp(kma_heap *h, size_t size, kma_tally *tl 
 		if (lane == leader && c >= 0 && served < gsize && !failed) {
 			tally(tl, KMA_T_ITER);
 			if (r.left == 0) {
-				if (!warp_reserve(h, (uint32_t)c, gsize - served, r, tl))
+				if (!warp_reserve(h, (uint32_t)c, gsize - served, r, tl, hint))
 					failed = true;
 			}
 			if (!failed) {

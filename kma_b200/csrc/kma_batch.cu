@@ -77,11 +77,12 @@ struct bt_counters {
 	unsigned long long fill, verify;
 };
 
-/* per-warp cache in shared memory: cnt[BT_NCLS] then slot[BT_NCLS][depth] */
+/* per-warp shared memory: cnt[BT_NCLS], hint[BT_NCLS], slot[BT_NCLS][depth] */
 struct bt_cache {
 	int *cnt;
 	uint32_t *slot;
 	uint32_t depth;
+	uint32_t *hint; /* the warp's kma_malloc_warp hint words */
 };
 
 /* Free q (NULL allowed) of n bytes: into the warp cache when it has room
@@ -134,7 +135,7 @@ __device__ __forceinline__ void *bt_malloc(kma_heap *h, const bt_cache &cc, uint
 			cc.cnt[lane] = 0;
 		__syncwarp();
 	}
-	void *q = kma_malloc_warp(h, need ? (size_t)n : ~(size_t)0);
+	void *q = kma_malloc_warp(h, need ? (size_t)n : ~(size_t)0, nullptr, cc.hint);
 	return need ? q : p;
 }
 
@@ -237,10 +238,13 @@ __global__ void __launch_bounds__(512, 2) k_bt_rounds(kma_heap *h, bt_dev w, uin
 	const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	bt_cache cc;
 	cc.depth = depth;
-	cc.cnt = bt_smem + wid * (BT_NCLS + BT_NCLS * depth);
-	cc.slot = reinterpret_cast<uint32_t *>(cc.cnt + BT_NCLS);
-	if (depth && lane < BT_NCLS)
+	cc.cnt = bt_smem + wid * (2 * BT_NCLS + BT_NCLS * depth);
+	cc.hint = reinterpret_cast<uint32_t *>(cc.cnt + BT_NCLS);
+	cc.slot = cc.hint + BT_NCLS;
+	if (lane < BT_NCLS) {
 		cc.cnt[lane] = 0;
+		cc.hint[lane] = 0;
+	}
 	__syncwarp();
 	bt_counters ct = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 	for (uint32_t r = 0; r <= w.rounds; r++) {
@@ -311,7 +315,7 @@ __global__ void k_bt_begin(bt_dev w)
 
 int bt_grid(uint32_t bd, uint32_t depth, int device, uint32_t *blocks, size_t *smem)
 {
-	*smem = (size_t)(bd / 32) * (BT_NCLS + BT_NCLS * depth) * 4;
+	*smem = (size_t)(bd / 32) * (2 * BT_NCLS + BT_NCLS * depth) * 4;
 	int per_sm = 0, sms = 0;
 	KMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bt_rounds, (int)bd, *smem));
 	KMA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));

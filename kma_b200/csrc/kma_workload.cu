@@ -63,9 +63,9 @@ __device__ __forceinline__ uint32_t c2_size(uint64_t d) { return 8u << (uint32_t
  * cycles per phase (malloc, tag fill, verify, free) -- a separate
  * instantiation, so the timed kernels carry none of it. */
 template <int MODE>
-__device__ __forceinline__ void *wl_malloc(kma_heap *h, size_t n, kma_tally *tl)
+__device__ __forceinline__ void *wl_malloc(kma_heap *h, size_t n, kma_tally *tl, uint32_t *hint)
 {
-	return (MODE & KMA_MODE_WARP) ? kma_malloc_warp(h, n, (MODE & KMA_MODE_PROFILE) ? tl : nullptr)
+	return (MODE & KMA_MODE_WARP) ? kma_malloc_warp(h, n, (MODE & KMA_MODE_PROFILE) ? tl : nullptr, hint)
 				      : kma_malloc(h, n);
 }
 template <int MODE>
@@ -81,6 +81,7 @@ struct wl_counters {
 	uint32_t mallocs, frees, nulls, bad, fill, verify;
 	unsigned long long cyc[4];
 	kma_tally tl;
+	uint32_t *hint; /* the warp's kma_malloc_warp hint words (shared memory), or NULL */
 };
 
 template <int MODE>
@@ -108,7 +109,7 @@ __device__ __forceinline__ void c1_round(kma_heap *h, uint32_t mask, uint32_t la
 	uint32_t n = c1_size(d);
 	void *p = NULL;
 	if (act) {
-		p = wl_malloc<MODE>(h, n, &ct.tl);
+		p = wl_malloc<MODE>(h, n, &ct.tl, ct.hint);
 		ct.mallocs++;
 		it.hash = hash_step(it.hash, p ? (int64_t)((unsigned char *)p - h->sb_base) : -1);
 		if (!p)
@@ -160,7 +161,7 @@ __device__ __forceinline__ void c2_round(kma_heap *h, const wl_dev &w, uint32_t 
 	}
 	void *p = NULL;
 	if (act) {
-		p = wl_malloc<MODE>(h, n, &ct.tl);
+		p = wl_malloc<MODE>(h, n, &ct.tl, ct.hint);
 		ct.mallocs++;
 		int64_t off = p ? (int64_t)((unsigned char *)p - h->sb_base) : -1;
 		it.hash = hash_step(it.hash, off);
@@ -287,7 +288,11 @@ __global__ void __launch_bounds__(256, 4) k_wl_rounds(kma_heap *h, wl_dev w, uin
 	const uint32_t lane = threadIdx.x & 31;
 	const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
 	const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}, {{0, 0, 0, 0, 0, 0, 0, 0}}};
+	__shared__ uint32_t s_hint[256 / 32][KMA_MAX_CLASSES];
+	if (lane < KMA_MAX_CLASSES)
+		s_hint[threadIdx.x >> 5][lane] = 0;
+	__syncwarp();
+	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}, {{0, 0, 0, 0, 0, 0, 0, 0}}, s_hint[threadIdx.x >> 5]};
 	const bool c2 = w.program == KMA_WL_C2;
 	{
 		for (uint32_t r = 0; r <= nrounds; r++) {
@@ -324,7 +329,7 @@ __global__ void k_wl_serial(kma_heap *h, wl_dev w, uint32_t nrounds, int round_m
 	if (blockIdx.x != 0 || threadIdx.x != 0)
 		return;
 	const uint32_t mask = 1u;
-	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}, {{0, 0, 0, 0, 0, 0, 0, 0}}};
+	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}, {{0, 0, 0, 0, 0, 0, 0, 0}}, nullptr};
 	if (!round_major) {
 		for (uint64_t g = 0; g < w.items; g++) {
 			wl_item it = {w.rng[g], w.hash[g], w.nlive[g]};
