@@ -72,13 +72,15 @@ typedef struct kma_batch_tune_entry {
 
 /* Autotuner: for every superblock size in sb_log2s (each a fresh heap of
  * heap_bytes on `device`), block dim in block_dims and cache depth in
- * depths, capture the run as a graph, launch it `warmup` times untimed and
+ * depths (heaps with at most `shards` class-table shards per class, 0 =
+ * the heap default), capture the run as a graph, launch it `warmup` times untimed and
  * `reps` times timed (CUDA events), and record the entry; *best is the
  * index of the configuration with the most successful calls per second
  * (mallocs that returned a block, plus frees) among those whose runs kept
  * every tag intact and set no heap error flag.
  * entries must hold n_sb * n_bd * n_depth entries. */
 int kma_batch_autotune(const kma_batch_job *jobs, uint32_t njobs, uint32_t rounds, uint64_t heap_bytes,
+		       uint32_t shards,
 		       const uint32_t *sb_log2s, uint32_t n_sb, const uint32_t *block_dims, uint32_t n_bd,
 		       const uint32_t *depths, uint32_t n_depth, uint32_t warmup, uint32_t reps, int device,
 		       kma_batch_tune_entry *entries, uint32_t *best);

@@ -193,7 +193,7 @@ SIGNATURES = [
     ("kma_batch_capture", c_int, [c_void_p, c_uint32, c_uint32, c_void_p]),
     ("kma_batch_launch", c_int, [c_void_p, c_void_p]),
     ("kma_batch_stats_get", c_int, [c_void_p, c_void_p, POINTER(KmaBatchStats)]),
-    ("kma_batch_autotune", c_int, [POINTER(KmaBatchJob), c_uint32, c_uint32, c_uint64, c_void_p, c_uint32,
+    ("kma_batch_autotune", c_int, [POINTER(KmaBatchJob), c_uint32, c_uint32, c_uint64, c_uint32, c_void_p, c_uint32,
                                    c_void_p, c_uint32, c_void_p, c_uint32, c_uint32, c_uint32, c_int,
                                    POINTER(KmaBatchTuneEntry), POINTER(c_uint32)]),
     # include/kma_graph.h

@@ -80,7 +80,7 @@ class Batch:
 
 
 def autotune(threads, seeds, rounds: int, heap_bytes: int, sb_log2s=(12, 14, 16), block_dims=(128, 256, 512),
-             depths=(0, 2, 4), warmup: int = 1, reps: int = 2, device: int = -1):
+             depths=(0, 2, 4), warmup: int = 1, reps: int = 2, device: int = -1, shards: int = 0):
     """Run the native autotuner; returns (entries, best index)."""
     jobs = _jobs(threads, seeds)
     sb = np.ascontiguousarray(sb_log2s, np.uint32)
@@ -89,7 +89,7 @@ def autotune(threads, seeds, rounds: int, heap_bytes: int, sb_log2s=(12, 14, 16)
     n = len(sb) * len(bd) * len(dp)
     ent = (KmaBatchTuneEntry * n)()
     best = c_uint32()
-    check(lib().kma_batch_autotune(jobs, len(jobs), rounds, heap_bytes, sb.ctypes.data, len(sb),
+    check(lib().kma_batch_autotune(jobs, len(jobs), rounds, heap_bytes, shards, sb.ctypes.data, len(sb),
                                    bd.ctypes.data, len(bd), dp.ctypes.data, len(dp), warmup, reps, device,
                                    ent, byref(best)), "kma_batch_autotune")
     out = []

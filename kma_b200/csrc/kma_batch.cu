@@ -521,7 +521,7 @@ extern "C" int kma_batch_stats_get(kma_batch_t b, void *stream, kma_batch_stats 
 }
 
 extern "C" int kma_batch_autotune(const kma_batch_job *jobs, uint32_t njobs, uint32_t rounds, uint64_t heap_bytes,
-		const uint32_t *sb_log2s, uint32_t n_sb, const uint32_t *block_dims, uint32_t n_bd,
+		uint32_t shards, const uint32_t *sb_log2s, uint32_t n_sb, const uint32_t *block_dims, uint32_t n_bd,
 		const uint32_t *depths, uint32_t n_depth, uint32_t warmup, uint32_t reps, int device,
 		kma_batch_tune_entry *entries, uint32_t *best)
 {
@@ -554,6 +554,7 @@ extern "C" int kma_batch_autotune(const kma_batch_job *jobs, uint32_t njobs, uin
 		cfg.sblocks = (uint32_t)(heap_bytes >> sb_log2s[i]);
 		cfg.sb_size_log2 = sb_log2s[i];
 		cfg.device = -1;
+		cfg.shards = shards;
 		kma_heap_t h = NULL;
 		rc = kma_create_ex(&cfg, st, &h);
 		if (rc != KMA_OK)
