@@ -200,4 +200,8 @@ def test_bounded_wait_times_out_without_fault():
             out = h.replay(np.array([[0, 16], [0, 8]], np.int64), mode)
             assert out[0] == -1  # class 2 (16 B): timed out
             assert out[1] >= 0   # class 1 unaffected
-            assert h.error_flags() & kma_b200.KMA_FLAG_TIMEOUT
+            flags = h.error_flags()
+            assert flags & kma_b200.KMA_FLAG_TIMEOUT
+            # and the flags name the wait: the per-thread reservation, or
+            # the warp path's reservation (KMA_ERR_AT_MALLOC / _AT_RESERVE)
+            assert flags & ((1 << 13) if mode == MODE_PLAIN else (1 << 15))
