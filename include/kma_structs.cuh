@@ -306,7 +306,7 @@ __device__ __forceinline__ kma_clqueue_item *kma_clqueue_next(const kma_clqueue_
 
 struct __align__(128) kma_iqueue {
 	unsigned char *base;
-	unsigned long long *dummies; /* link words of the internal dummies [nshards-1] */
+	unsigned long long *dummies; /* link words of the internal dummies [nshards-1], then the nil word */
 	kma_line64 *ends;            /* shard k: head at ends[2k], tail at ends[2k+1] */
 	uint32_t stride_l2;
 	uint32_t capacity;   /* user items are 1..capacity */
@@ -318,6 +318,10 @@ struct __align__(128) kma_iqueue {
 namespace kma_detail {
 __device__ __forceinline__ unsigned long long *iq_link(const kma_iqueue *q, uint32_t idx)
 {
+	/* index 0 (no item) has no link: a read of it sees the nil word (0),
+	 * so no state can address outside the item array */
+	if (idx == 0)
+		return &q->dummies[q->nshards - 1];
 	if (idx > q->capacity)
 		return &q->dummies[idx - q->capacity - 1];
 	return reinterpret_cast<unsigned long long *>(q->base + ((size_t)(idx - 1) << q->stride_l2));
@@ -405,11 +409,8 @@ __device__ inline void *kma_iqueue_dequeue_shard(kma_iqueue *q, uint32_t shard)
 			cas64_acqrel(tailw, t, tw_make(tw_tag(t) + 1, tw_idx(n)));
 		} else if (cas64_acqrel(headw, hd, tw_make(tw_tag(hd) + 1, tw_idx(n))) == hd) {
 			uint32_t idx = tw_idx(hd);
-			if (idx > q->capacity) {
-				/* an internal dummy left the shard: take the next one */
-				it = 0;
-				continue;
-			}
+			if (idx > q->capacity)
+				continue; /* an internal dummy left the shard: take the next item */
 			return kma_iqueue_item(q, idx);
 		}
 		backoff(it);
