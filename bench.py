@@ -345,7 +345,7 @@ def run_ours(args) -> int:
                               "step_ms": [round(x, 3) for x in step_ms],
                               "rounds_ms": [round(x, 3) for x in rounds_ms],
                               "ops_per_step": st["mallocs"] + st["frees"], "nulls": st["nulls"],
-                              "bad_tags": st["bad_tags"],
+                              "bad_tags": st["bad_tags"], "step_error_flags": step_flags,
                               "rounds_launch_bytes_per_step": None}))
         wl.close()
         heap.close()
@@ -475,7 +475,9 @@ def run_ours(args) -> int:
                        "class_shards": heap.cls_shards,
                        "rounds_phase_share": phase_share,
                        "malloc_tally": tally,
-                       "warp_over_plain": round(value / world / plain, 2) if plain else None},
+                       "warp_over_plain": round(value / world / plain, 2) if plain else None,
+                       "warp_over_plain_default_heap":
+                           round(value / world / plain_default, 2) if plain_default else None},
             "roofline": {"bound": "hbm", "kernel": "k_wl_rounds<warp>",
                          "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": round(achieved / pk["hbm_gbs"], 4), "traffic": traffic,

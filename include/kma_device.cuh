@@ -142,6 +142,12 @@ __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t *p)
 	asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
 	return v;
 }
+__device__ __forceinline__ uint32_t ld_relaxed16(const uint16_t *p)
+{
+	uint16_t v;
+	asm volatile("ld.relaxed.gpu.global.u16 %0, [%1];" : "=h"(v) : "l"(p) : "memory");
+	return v;
+}
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p)
 {
 	uint32_t v;
@@ -543,6 +549,23 @@ __device__ __forceinline__ void sb_format(kma_heap *h, uint32_t s, uint32_t c, u
 /* ------------------------------------------------------------------ */
 namespace kma_detail {
 
+/* A class slot that names a superblock which cannot serve its class (no
+ * free count left, or recycled for another class) is cleared by the
+ * thread that finds it, not waited on.  The thread that takes a
+ * superblock's last slots clears the slot it read the superblock from;
+ * if the superblock was recycled meanwhile and republished in another
+ * shard's slot of the same class, that slot keeps naming it, full, until
+ * all its blocks are freed -- and the threads waiting on that slot may be
+ * the ones holding them.  Clearing at worst hides a superblock whose
+ * slots were freed again since the read; it returns to the free list
+ * when all its blocks are freed, as any detached one.  One-thread
+ * execution never finds such a slot (a taker always clears the slot it
+ * read), so serial replay is unchanged. */
+__device__ __forceinline__ void clear_stale(uint32_t *clsw, uint32_t cur)
+{
+	cas_relaxed(clsw, cur, 0);
+}
+
 /* kma.cl:232-273: claim a bitmap bit at or above `hint` (wrapping),
  * write the hint into word 0 of the block. */
 __device__ __forceinline__ void *sb_get_block(kma_heap *h, uint32_t s, uint32_t c, uint32_t hint)
@@ -619,8 +642,10 @@ __device__ inline void *kma_malloc(kma_heap *h, size_t size)
 		uint32_t *stp = &h->sb_state[s];
 		/* kma.cl:198 reads the state with atom_add(.., 0) */
 		uint32_t st = atomicAdd(stp, 0u);
-		if (st_class(st) != (uint32_t)c || st_free(st) == 0)
+		if (st_class(st) != (uint32_t)c || st_free(st) == 0) {
+			clear_stale(clsw, cur);
 			continue;
+		}
 		uint32_t fr = st_free(st) - 1;
 		if (cas_relaxed(stp, st, st - 1) != st)
 			continue;
@@ -654,7 +679,16 @@ __device__ __forceinline__ bool block_locate(const kma_heap *h, const void *p, u
  * free: kma.cl:362-367. */
 __device__ __forceinline__ void sb_recycle(kma_heap *h, uint32_t s, uint32_t c)
 {
-	uint32_t home = h->sb_home[s];
+	/* The home shard of this incarnation was stored before the release
+	 * that published its state (sb_format).  This load issues only after
+	 * the caller's CAS on that state has returned (it decides whether to
+	 * recycle), and a gpu-scope relaxed load is served at L2, where that
+	 * store already was: it sees the current home.  A plain load may be
+	 * served from this SM's L1, where a line of sb_home read during an
+	 * earlier incarnation can still sit: the slot of the old home would be
+	 * cleared and the current one left naming a superblock on the free
+	 * list. */
+	uint32_t home = ld_relaxed16(&h->sb_home[s]);
 	cas_relaxed(cls_word(h, c, home), s + KMA_CLS_BASE, 0);
 	sb_enqueue(h, s);
 }
@@ -859,11 +893,16 @@ __device__ __forceinline__ int warp_reserve(kma_heap *h, uint32_t c, uint32_t wa
 		}
 		uint32_t s = cur - KMA_CLS_BASE;
 		uint32_t *stp = &h->sb_state[s];
-		uint32_t st = cur == guess ? st_guess : ld_relaxed(stp);
+		const bool speculated = cur == guess;
+		uint32_t st = speculated ? st_guess : ld_relaxed(stp);
 		guess = cur;
 		if (st_class(st) != c || st_free(st) == 0) {
 			tally(tl, KMA_T_STALE);
-			backoff(it);
+			/* the speculative state load may be older than cur */
+			if (speculated)
+				st = ld_relaxed(stp);
+			if (st_class(st) != c || st_free(st) == 0)
+				clear_stale(clsw, cur);
 			continue;
 		}
 		uint32_t fr = st_free(st);

@@ -154,18 +154,21 @@ __device__ __forceinline__ void bt_round(kma_heap *h, const bt_dev &w, const bt_
 	for (uint32_t i = 0; i < (act ? nl : 0u); i++)
 		if ((w.meta[(uint64_t)i * items + g] >> 16) <= r || r == w.rounds)
 			emask |= 1u << i;
-	uint32_t npass = __reduce_max_sync(mask, (uint32_t)__popc(emask));
-	uint32_t rest = emask;
-	for (uint32_t pass = 0; pass < npass; pass++) {
+	/* the warp's ending blocks, packed 32 to a pass (warp_pack); each is
+	 * verified against its owner's tag by the lane that takes it */
+	const warp_pack wp = warp_pack_init(lane, emask);
+	for (uint32_t base = 0; base < wp.total; base += 32) {
+		uint32_t owner, i;
+		const bool mine = warp_pack_slot(wp, lane, base, owner, i);
+		const uint64_t o_g = __shfl_sync(mask, g, owner);
 		void *q = NULL;
 		uint32_t qn = 0;
-		if (rest) {
-			uint32_t i = __ffs(rest) - 1;
-			rest &= rest - 1;
-			q = bt_block(h, w.off4[(uint64_t)i * items + g]);
-			qn = bt_bytes(w.meta[(uint64_t)i * items + g]);
+		if (mine) {
+			const uint64_t e = (uint64_t)i * items + o_g;
+			q = bt_block(h, w.off4[e]);
+			qn = bt_bytes(w.meta[e]);
 		}
-		if (coop_verify(mask, lane, q, qn, tag))
+		if (coop_verify(mask, lane, q, qn, (uint32_t)o_g))
 			ct.bad++;
 		bt_free(h, cc, lane, q, qn, ct);
 		if (q) {
@@ -173,6 +176,8 @@ __device__ __forceinline__ void bt_round(kma_heap *h, const bt_dev &w, const bt_
 			ct.verify += qn;
 		}
 	}
+	/* other lanes read this lane's table above; it is compacted next */
+	__syncwarp(mask);
 	if (emask) {
 		uint32_t j = 0;
 		for (uint32_t i = 0; i < nl; i++) {

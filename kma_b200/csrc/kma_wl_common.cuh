@@ -115,6 +115,74 @@ __device__ __forceinline__ bool coop_verify(uint32_t mask, uint32_t lane, const 
 	return bad != 0 || ((badbits >> lane) & 1u);
 }
 
+/* Position of the (k+1)-th set bit of m; requires k < popc(m). */
+__device__ __forceinline__ uint32_t nth_bit(uint32_t m, uint32_t k)
+{
+	uint32_t pos = 0;
+#pragma unroll
+	for (uint32_t s = 16; s; s >>= 1) {
+		uint32_t lo = __popc(m & ((1u << s) - 1u));
+		if (k >= lo) {
+			k -= lo;
+			m >>= s;
+			pos += s;
+		}
+	}
+	return pos;
+}
+
+/* Packed numbering of a full warp's work bits: the set bits of every
+ * lane's `bits`, in lane order and within a lane in increasing bit index,
+ * are numbered 0..total-1 by a warp prefix sum, so that pass k serves
+ * numbers 32k..32k+31 with lane l taking number 32k+l.  Used for the
+ * frees of a round: one pass per set bit of the busiest lane would leave
+ * most lanes idle through about twice as many passes, each a chain of
+ * dependent round trips (table load, payload loads, free atomics). */
+struct warp_pack {
+	uint32_t bits, excl, incl, total;
+};
+
+/* Every lane of the warp calls it. */
+__device__ __forceinline__ warp_pack warp_pack_init(uint32_t lane, uint32_t bits)
+{
+	warp_pack wp;
+	wp.bits = bits;
+	const uint32_t c = __popc(bits);
+	uint32_t incl = c;
+#pragma unroll
+	for (uint32_t o = 1; o < 32; o <<= 1) {
+		uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+		if (lane >= o)
+			incl += v;
+	}
+	wp.incl = incl;
+	wp.excl = incl - c;
+	wp.total = __shfl_sync(0xffffffffu, incl, 31);
+	return wp;
+}
+
+/* Lane `lane`'s number in the pass starting at `base` (a multiple of 32
+ * below total): true with the lane that owns it and its bit index, or
+ * false (owner = lane) when the pass has no number for this lane.  Every
+ * lane of the warp calls it. */
+__device__ __forceinline__ bool warp_pack_slot(const warp_pack &wp, uint32_t lane, uint32_t base, uint32_t &owner,
+		uint32_t &bit)
+{
+	const uint32_t full = 0xffffffffu;
+	/* lanes owning numbers in this pass, and the pass slot of each one's
+	 * first number (distinct slots, increasing with the lane) */
+	const bool in = wp.incl > wp.excl && wp.excl < base + 32 && wp.incl > base;
+	const uint32_t lanes = __ballot_sync(full, in);
+	const uint32_t starts = __reduce_or_sync(full, in ? 1u << (wp.excl > base ? wp.excl - base : 0u) : 0u);
+	const uint32_t s = base + lane;
+	const bool mine = s < wp.total;
+	owner = mine ? nth_bit(lanes, __popc(starts & (full >> (31 - lane))) - 1) : lane;
+	const uint32_t o_excl = __shfl_sync(full, wp.excl, owner);
+	const uint32_t o_bits = __shfl_sync(full, wp.bits, owner);
+	bit = mine ? nth_bit(o_bits, s - o_excl) : 0u;
+	return mine;
+}
+
 } /* namespace kma_wl */
 
 #endif /* KMA_WL_COMMON_CUH */

@@ -127,6 +127,40 @@ __device__ __forceinline__ void c1_round(kma_heap *h, uint32_t mask, uint32_t la
 	}
 }
 
+/* The whole warp's frees of one C2 round (bit i of a lane's fmask: entry
+ * i of its live table), packed 32 to a pass (warp_pack); each block is
+ * verified against its owner's tag and freed by the lane that takes it. */
+template <int MODE>
+__device__ __forceinline__ void c2_free_packed(kma_heap *h, const wl_dev &w, uint32_t lane, uint64_t g,
+		uint32_t fmask, wl_counters &ct, long long &t0)
+{
+	const uint32_t full = 0xffffffffu;
+	const warp_pack wp = warp_pack_init(lane, fmask);
+	for (uint32_t base = 0; base < wp.total; base += 32) {
+		uint32_t owner, i;
+		const bool mine = warp_pack_slot(wp, lane, base, owner, i);
+		const uint64_t o_g = __shfl_sync(full, g, owner);
+		void *q = NULL;
+		uint32_t qn = 0;
+		if (mine) {
+			const uint64_t e = (uint64_t)i * w.items + o_g;
+			q = h->sb_base + w.live_off[e];
+			qn = w.live_size[e];
+		}
+		if (coop_verify(full, lane, q, qn, (uint32_t)o_g))
+			ct.bad++;
+		phase<MODE>(ct, 2, t0);
+		wl_free<MODE>(h, q);
+		phase<MODE>(ct, 3, t0);
+		if (q) {
+			ct.frees++;
+			ct.verify += qn;
+		}
+	}
+	/* other lanes read this lane's live table above; it is compacted next */
+	__syncwarp(full);
+}
+
 /* C2 round */
 template <int MODE>
 __device__ __forceinline__ void c2_round(kma_heap *h, const wl_dev &w, uint32_t mask, uint32_t lane, bool act,
@@ -180,11 +214,15 @@ __device__ __forceinline__ void c2_round(kma_heap *h, const wl_dev &w, uint32_t 
 	phase<MODE>(ct, 1, t0);
 	uint64_t bits = splitmix(it.rng);
 	uint32_t nl = act ? it.nlive : 0;
-	/* live entry i is freed this round when bit i of the draw is set; the
-	 * warp makes one pass per freed block of its busiest lane, each lane
-	 * freeing its entries in increasing i */
+	/* live entry i is freed this round when bit i of the draw is set.  A
+	 * full warp packs its frees (c2_free_packed); a partial one (the
+	 * one-thread serial replay) makes one pass per freed block of its
+	 * busiest lane, each lane freeing its entries in increasing i, the
+	 * oracle's order */
 	uint32_t fmask = nl ? ((uint32_t)bits & (nl >= 32 ? 0xffffffffu : ((1u << nl) - 1u))) : 0u;
-	uint32_t npass = __reduce_max_sync(mask, (uint32_t)__popc(fmask));
+	uint32_t npass = mask == 0xffffffffu ? 0u : __reduce_max_sync(mask, (uint32_t)__popc(fmask));
+	if (mask == 0xffffffffu)
+		c2_free_packed<MODE>(h, w, lane, g, fmask, ct, t0);
 	uint32_t rest = fmask;
 	for (uint32_t pass = 0; pass < npass; pass++) {
 		void *q = NULL;

@@ -191,6 +191,24 @@ def test_double_free_is_refused_not_corrupting():
             assert ins.check_canonical_empty(img, h.bitmaps()) == []
 
 
+@pytest.mark.parametrize("heap", HEAPS, ids=HEAP_IDS)
+@pytest.mark.parametrize("mode", MODES, ids=MODE_IDS)
+def test_stale_class_slot_is_cleared_not_waited_on(mode, heap):
+    # a class slot naming a superblock that cannot serve the class (here one
+    # formatted for another class; concurrently, one whose last slots were
+    # taken through another shard's slot after a recycle): the request
+    # clears the slot and refills instead of waiting out the spin limit
+    with Heap(32, 12, spin_limit=2000, **heap) as h:
+        a = h.replay(np.array([[0, 8]], np.int64), mode)  # a class-1 superblock
+        assert a[0] >= 0
+        s = int(a[0]) >> 12
+        h.debug_set_class_word(2, s + 2)  # KMA_CLS_BASE + s, in every shard
+        out = h.replay(np.array([[0, 16], [0, 16], [1, 0], [1, 1]], np.int64), mode)
+        assert (out[:2] >= 0).all()
+        assert ((out[:2] >> 12) != s).all()
+        assert h.error_flags() == 0
+
+
 def test_bounded_wait_times_out_without_fault():
     # a class word stuck at POISON (nothing will clear it): every request
     # of that class gives up after spin_limit iterations and returns NULL
