@@ -134,6 +134,62 @@ int kma_snapshot(kma_heap_t h, void *stream, uint32_t *cls, uint32_t *state,
  * words = ceil(slots of class 0 / 32).  Device pointer dst. */
 int kma_gather_bitmaps(kma_heap_t h, void *stream, uint32_t *dst_dev, uint32_t words);
 
+/* ---- heap images: save and restore ------------------------------------- */
+/* A heap image is a position-independent copy of a heap's whole state: the
+ * class table, the per-superblock state and home shard, the free list and
+ * the superblock region (blocks, residue words and bitmaps).  Every link
+ * the heap keeps is a superblock index or an offset from the first
+ * superblock, so an image loads into any heap of the same geometry -- in
+ * another process, on another GPU, at another address -- and the loaded
+ * heap hands out the same offsets the saved one would have.  (Pointers
+ * that callers stored inside their blocks are theirs to relocate.)  The
+ * reference has no counterpart; its heap is one cl_mem buffer a host can
+ * only copy verbatim into the same context.
+ *
+ * Layout (little-endian): this header, then the sections at the offsets it
+ * gives, each 256-byte aligned:
+ *   off_cls     u32[cls_lines]  class words, class-major (0 empty, s+2
+ *                               superblock s; see kma_snapshot)
+ *   off_state   u32[sblocks]    class<<28 | slots<<14 | free
+ *   off_home    u16[sblocks]    home shard of each superblock
+ *   off_flist   u64[flist_words] free-list words: ring slots {seq:32 | sb:32}
+ *                               (ring != 0) or MS-queue links {tag:32 | idx+1:32}
+ *   off_region  u8[sblocks << sb_log2] the superblocks */
+#define KMA_IMAGE_MAGIC "KMAHEAP1"
+#define KMA_IMAGE_VERSION 1u
+typedef struct kma_image_header {
+	char magic[8];            /* KMA_IMAGE_MAGIC, no terminator */
+	uint32_t version;         /* KMA_IMAGE_VERSION */
+	uint32_t header_bytes;    /* sizeof(kma_image_header) */
+	uint32_t sb_log2, sblocks, pages;
+	uint32_t ring;            /* 1: ticket-ring free list, 0: MS queue */
+	uint32_t nclasses, cls_lines, flist_words;
+	uint32_t err;             /* the heap's KMA_FLAG_* word */
+	uint64_t free_head, free_tail; /* ring tickets, or MS-queue {tag | idx+1} words */
+	uint32_t ring_avail, reserved;
+	uint32_t cls_shards[16];  /* shards of each class (nclasses used) */
+	uint64_t off_cls, off_state, off_home, off_flist, off_region;
+	uint64_t total_bytes;     /* the image's size */
+} kma_image_header;
+
+/* Bytes an image of h takes (header, metadata and the superblock region). */
+int kma_image_bytes(kma_heap_t h, uint64_t *bytes);
+/* Write an image of h to dst (host or device memory, dst_bytes >=
+ * kma_image_bytes), stream-ordered after earlier work on `stream`, and
+ * wait for it.  The heap must be quiescent: no kernel on any stream may
+ * use it meanwhile (an image with a refill in flight is refused by
+ * kma_image_load).  KMA_EINVAL if dst_bytes is too small. */
+int kma_image_save(kma_heap_t h, void *stream, void *dst, uint64_t dst_bytes);
+/* Replace h's whole state with the image at src (host or device memory),
+ * stream-ordered, and wait for it.  h keeps its own spin limit.  Returns
+ * KMA_EINVAL, leaving h unchanged, when the image is truncated, of another
+ * version, of a heap of other geometry (superblock size, superblocks,
+ * free-list kind, shards per class), or holds any word that could address
+ * outside the heap (a class word, a free-list entry or a home shard out of
+ * range, a state with an unknown class or more free than slots, a refill
+ * in flight). */
+int kma_image_load(kma_heap_t h, void *stream, const void *src, uint64_t src_bytes);
+
 /* ---- serial replay ---------------------------------------------------- */
 /* One-thread-at-a-time replay of an op stream on the device:
  * ops[2i] = kind, ops[2i+1] = arg; kind 0 = malloc(arg) -> out[i] = offset

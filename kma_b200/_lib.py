@@ -133,6 +133,9 @@ SIGNATURES = [
     ("kma_snapshot", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                              c_uint64, c_uint64, c_void_p]),
     ("kma_gather_bitmaps", c_int, [c_void_p, c_void_p, c_void_p, c_uint32]),
+    ("kma_image_bytes", c_int, [c_void_p, POINTER(c_uint64)]),
+    ("kma_image_save", c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
+    ("kma_image_load", c_int, [c_void_p, c_void_p, c_void_p, c_uint64]),
     ("kma_replay", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int, c_void_p]),
     ("kma_replay_host", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_int]),
     ("kma_wl_create", c_int, [c_void_p, c_int, c_uint64, POINTER(c_void_p)]),

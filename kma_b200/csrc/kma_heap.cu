@@ -539,3 +539,189 @@ extern "C" int kma_debug_set_class_word(kma_heap_t h, uint32_t cls, uint32_t val
 	KMA_CUDA(cudaStreamSynchronize(st));
 	return KMA_OK;
 }
+
+/* ------------------------------------------------------------------ */
+/* heap images (kma.h): save and restore                               */
+/* ------------------------------------------------------------------ */
+namespace {
+
+const uint64_t KMA_IMG_ALIGN = 256;
+static_assert(sizeof(kma_image_header) == 184, "kma_image_header is packed, 184 bytes");
+
+/* The image layout of heap geometry hh (sections 256-byte aligned). */
+void kma_image_layout(const kma_heap &hh, kma_image_header &hdr)
+{
+	memset(&hdr, 0, sizeof(hdr));
+	memcpy(hdr.magic, KMA_IMAGE_MAGIC, 8);
+	hdr.version = KMA_IMAGE_VERSION;
+	hdr.header_bytes = sizeof(kma_image_header);
+	hdr.sb_log2 = hh.sb_log2;
+	hdr.sblocks = hh.nsb;
+	hdr.pages = hh.pages;
+	hdr.ring = (hh.flags & KMA_HEAP_RING) ? 1u : 0u;
+	hdr.nclasses = hh.nclasses;
+	hdr.cls_lines = hh.cls_lines;
+	hdr.flist_words = hdr.ring ? hh.ring_cap : hh.nsb;
+	for (uint32_t c = 0; c < hh.nclasses && c < 16; c++)
+		hdr.cls_shards[c] = hh.cls_nsh[c];
+	uint64_t o = kma_align_up(sizeof(kma_image_header), KMA_IMG_ALIGN);
+	hdr.off_cls = o;
+	o = kma_align_up(o + (uint64_t)hdr.cls_lines * 4, KMA_IMG_ALIGN);
+	hdr.off_state = o;
+	o = kma_align_up(o + (uint64_t)hdr.sblocks * 4, KMA_IMG_ALIGN);
+	hdr.off_home = o;
+	o = kma_align_up(o + (uint64_t)hdr.sblocks * 2, KMA_IMG_ALIGN);
+	hdr.off_flist = o;
+	o = kma_align_up(o + (uint64_t)hdr.flist_words * 8, KMA_IMG_ALIGN);
+	hdr.off_region = o;
+	hdr.total_bytes = o + hh.region_bytes;
+}
+
+/* Every metadata word of an image stays inside the heap: what a kernel
+ * would index with it (sb_state, sb_next, ring slots, class lines) is in
+ * range.  Region bytes need no check: bitmap bits only select slots below
+ * a class's slot count. */
+bool kma_image_valid(const kma_heap &hh, const kma_image_header &hdr, const uint32_t *cls,
+		const uint32_t *state, const uint16_t *home, const unsigned long long *fl)
+{
+	const uint32_t nsb = hh.nsb;
+	for (uint32_t i = 0; i < hdr.cls_lines; i++)
+		if (cls[i] == KMA_POISON || (cls[i] >= KMA_CLS_BASE && cls[i] - KMA_CLS_BASE >= nsb))
+			return false;
+	for (uint32_t s = 0; s < nsb; s++) {
+		uint32_t st = state[s];
+		if (st == 0)
+			continue;
+		uint32_t c = st >> KMA_ST_CLASS_SHIFT;
+		uint32_t slots = (st >> KMA_ST_SLOTS_SHIFT) & KMA_ST_FREE_MASK;
+		uint32_t fr = st & KMA_ST_FREE_MASK;
+		if (c >= hh.nclasses || slots != hh.cls_slots[c] || fr > slots || home[s] >= hh.cls_nsh[c])
+			return false;
+	}
+	if (hdr.ring) {
+		if (hdr.free_tail < hdr.free_head || hdr.free_tail - hdr.free_head > hh.ring_cap)
+			return false;
+		int32_t avail = (int32_t)hdr.ring_avail;
+		if (avail > (int32_t)hh.ring_cap || avail < -(int32_t)hh.ring_cap)
+			return false;
+		for (uint32_t i = 0; i < hdr.flist_words; i++)
+			if ((uint32_t)fl[i] >= nsb)
+				return false;
+	} else {
+		uint32_t hi = (uint32_t)hdr.free_head, ti = (uint32_t)hdr.free_tail;
+		if (hi == 0 || hi > nsb || ti == 0 || ti > nsb)
+			return false;
+		for (uint32_t i = 0; i < hdr.flist_words; i++)
+			if ((uint32_t)fl[i] > nsb)
+				return false;
+	}
+	return true;
+}
+
+} /* namespace */
+
+extern "C" int kma_image_bytes(kma_heap_t h, uint64_t *bytes)
+{
+	if (!h || !bytes)
+		return KMA_EINVAL;
+	kma_image_header hdr;
+	kma_image_layout(h->hh, hdr);
+	*bytes = hdr.total_bytes;
+	return KMA_OK;
+}
+
+extern "C" int kma_image_save(kma_heap_t h, void *stream, void *dst, uint64_t dst_bytes)
+{
+	if (!h || !dst)
+		return KMA_EINVAL;
+	kma_image_header hdr;
+	kma_image_layout(h->hh, hdr);
+	if (dst_bytes < hdr.total_bytes)
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	if (!g.ok)
+		return KMA_ENODEV;
+	cudaStream_t st = kma_stream(stream);
+	/* the hot words and the class lines live in the device header */
+	std::vector<unsigned char> dev_hdr(sizeof(kma_heap));
+	kma_heap *tmp = reinterpret_cast<kma_heap *>(dev_hdr.data());
+	KMA_CUDA(cudaMemcpyAsync(tmp, h->dh, sizeof(kma_heap), cudaMemcpyDeviceToHost, st));
+	KMA_CUDA(cudaStreamSynchronize(st));
+	hdr.free_head = tmp->free_head.v;
+	hdr.free_tail = tmp->free_tail.v;
+	hdr.ring_avail = tmp->ring_avail.v;
+	hdr.err = tmp->err.v;
+	std::vector<uint32_t> cls(hdr.cls_lines);
+	for (uint32_t i = 0; i < hdr.cls_lines; i++)
+		cls[i] = tmp->cls[i].v;
+	unsigned char *d = static_cast<unsigned char *>(dst);
+	const unsigned long long *fl = hdr.ring ? h->hh.ring : h->hh.sb_next;
+	KMA_CUDA(cudaMemcpyAsync(d, &hdr, sizeof(hdr), cudaMemcpyDefault, st));
+	KMA_CUDA(cudaMemcpyAsync(d + hdr.off_cls, cls.data(), (size_t)hdr.cls_lines * 4, cudaMemcpyDefault, st));
+	KMA_CUDA(cudaMemcpyAsync(d + hdr.off_state, h->hh.sb_state, (size_t)hdr.sblocks * 4, cudaMemcpyDefault, st));
+	KMA_CUDA(cudaMemcpyAsync(d + hdr.off_home, h->hh.sb_home, (size_t)hdr.sblocks * 2, cudaMemcpyDefault, st));
+	KMA_CUDA(cudaMemcpyAsync(d + hdr.off_flist, fl, (size_t)hdr.flist_words * 8, cudaMemcpyDefault, st));
+	KMA_CUDA(cudaMemcpyAsync(d + hdr.off_region, h->hh.sb_base, h->hh.region_bytes, cudaMemcpyDefault, st));
+	KMA_CUDA(cudaStreamSynchronize(st)); /* the staged header and class words */
+	return KMA_OK;
+}
+
+extern "C" int kma_image_load(kma_heap_t h, void *stream, const void *src, uint64_t src_bytes)
+{
+	if (!h || !src)
+		return KMA_EINVAL;
+	kma_image_header want;
+	kma_image_layout(h->hh, want);
+	if (src_bytes < sizeof(kma_image_header))
+		return KMA_EINVAL;
+	kma_device_guard g(h->device);
+	if (!g.ok)
+		return KMA_ENODEV;
+	cudaStream_t st = kma_stream(stream);
+	const unsigned char *s = static_cast<const unsigned char *>(src);
+	kma_image_header hdr;
+	KMA_CUDA(cudaMemcpyAsync(&hdr, s, sizeof(hdr), cudaMemcpyDefault, st));
+	KMA_CUDA(cudaStreamSynchronize(st));
+	/* same format and geometry: every section offset then matches too */
+	if (memcmp(hdr.magic, want.magic, 8) || hdr.version != want.version ||
+			hdr.header_bytes != want.header_bytes || hdr.sb_log2 != want.sb_log2 ||
+			hdr.sblocks != want.sblocks || hdr.pages != want.pages || hdr.ring != want.ring ||
+			hdr.nclasses != want.nclasses || hdr.cls_lines != want.cls_lines ||
+			hdr.flist_words != want.flist_words ||
+			memcmp(hdr.cls_shards, want.cls_shards, sizeof(want.cls_shards)) ||
+			hdr.off_cls != want.off_cls || hdr.off_state != want.off_state ||
+			hdr.off_home != want.off_home || hdr.off_flist != want.off_flist ||
+			hdr.off_region != want.off_region || hdr.total_bytes != want.total_bytes ||
+			src_bytes < hdr.total_bytes)
+		return KMA_EINVAL;
+	/* the metadata comes to the host for checking before any of it reaches
+	 * the device */
+	std::vector<uint32_t> cls(hdr.cls_lines), state(hdr.sblocks);
+	std::vector<uint16_t> home(hdr.sblocks);
+	std::vector<unsigned long long> fl(hdr.flist_words);
+	KMA_CUDA(cudaMemcpyAsync(cls.data(), s + hdr.off_cls, cls.size() * 4, cudaMemcpyDefault, st));
+	KMA_CUDA(cudaMemcpyAsync(state.data(), s + hdr.off_state, state.size() * 4, cudaMemcpyDefault, st));
+	KMA_CUDA(cudaMemcpyAsync(home.data(), s + hdr.off_home, home.size() * 2, cudaMemcpyDefault, st));
+	KMA_CUDA(cudaMemcpyAsync(fl.data(), s + hdr.off_flist, fl.size() * 8, cudaMemcpyDefault, st));
+	std::vector<unsigned char> dev_hdr(sizeof(kma_heap));
+	kma_heap *tmp = reinterpret_cast<kma_heap *>(dev_hdr.data());
+	KMA_CUDA(cudaMemcpyAsync(tmp, h->dh, sizeof(kma_heap), cudaMemcpyDeviceToHost, st));
+	KMA_CUDA(cudaStreamSynchronize(st));
+	if (!kma_image_valid(h->hh, hdr, cls.data(), state.data(), home.data(), fl.data()))
+		return KMA_EINVAL;
+	tmp->free_head.v = hdr.free_head;
+	tmp->free_tail.v = hdr.free_tail;
+	tmp->ring_avail.v = hdr.ring_avail;
+	tmp->err.v = hdr.err;
+	for (uint32_t i = 0; i < hdr.cls_lines; i++)
+		tmp->cls[i].v = cls[i];
+	unsigned long long *dfl = hdr.ring ? h->hh.ring : h->hh.sb_next;
+	KMA_CUDA(cudaMemcpyAsync(h->hh.sb_state, state.data(), state.size() * 4, cudaMemcpyHostToDevice, st));
+	KMA_CUDA(cudaMemcpyAsync(h->hh.sb_home, home.data(), home.size() * 2, cudaMemcpyHostToDevice, st));
+	KMA_CUDA(cudaMemcpyAsync(dfl, fl.data(), fl.size() * 8, cudaMemcpyHostToDevice, st));
+	KMA_CUDA(cudaMemcpyAsync(h->hh.sb_base, s + hdr.off_region, h->hh.region_bytes, cudaMemcpyDefault, st));
+	/* the device header last: its geometry fields are h's own, read back above */
+	KMA_CUDA(cudaMemcpyAsync(h->dh, tmp, sizeof(kma_heap), cudaMemcpyHostToDevice, st));
+	KMA_CUDA(cudaStreamSynchronize(st));
+	return KMA_OK;
+}

@@ -7,7 +7,7 @@ the C1/C2 stress programs; both only ever call the CUDA library.
 from __future__ import annotations
 
 import ctypes
-from ctypes import byref, c_float, c_uint32, c_void_p
+from ctypes import byref, c_float, c_uint32, c_uint64, c_void_p
 
 import numpy as np
 
@@ -152,6 +152,38 @@ class Heap:
                          nclasses=self.nclasses, cls_size=list(self.cls_size),
                          cls_slots=list(self.cls_slots), cls_raw=cls, cls_shards=list(self.cls_shards),
                          state=state, freelist=freelist, region=reg if region else None)
+
+    def image_bytes(self) -> int:
+        """Size of a heap image (kma_image_bytes)."""
+        n = c_uint64()
+        check(lib().kma_image_bytes(self.handle, byref(n)), "kma_image_bytes")
+        return int(n.value)
+
+    def image_save(self, dst_ptr: int | None = None, dst_bytes: int = 0, stream=None):
+        """Save a position-independent image of the heap (kma_image_save):
+        into host or device memory at dst_ptr, or, with no pointer, into a
+        new host numpy uint8 array, which is returned.  The heap must be
+        quiescent."""
+        if dst_ptr is None:
+            buf = np.zeros(self.image_bytes(), np.uint8)
+            check(lib().kma_image_save(self.handle, _stream_ptr(stream), buf.ctypes.data, buf.nbytes),
+                  "kma_image_save")
+            return buf
+        check(lib().kma_image_save(self.handle, _stream_ptr(stream), dst_ptr, dst_bytes), "kma_image_save")
+        return None
+
+    def image_load(self, src, src_bytes: int | None = None, stream=None) -> None:
+        """Replace the heap's state with an image (kma_image_load): a numpy
+        uint8 array, or a host/device address with its size.  KmaError
+        (KMA_EINVAL) for an image of other geometry or one that does not
+        validate; the heap is then unchanged."""
+        if isinstance(src, np.ndarray):
+            src = np.ascontiguousarray(src, np.uint8)
+            check(lib().kma_image_load(self.handle, _stream_ptr(stream), src.ctypes.data, src.nbytes),
+                  "kma_image_load")
+            return
+        check(lib().kma_image_load(self.handle, _stream_ptr(stream), int(src), int(src_bytes)),
+              "kma_image_load")
 
     # -- serial replay ------------------------------------------------------
     def replay(self, ops: np.ndarray, mode: int = _lib.MODE_PLAIN) -> np.ndarray:

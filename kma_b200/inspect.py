@@ -79,6 +79,68 @@ def decode(img: HeapImage) -> Canonical:
     return canon
 
 
+IMAGE_MAGIC = b"KMAHEAP1"
+IMAGE_HEADER = np.dtype([
+    ("magic", "S8"), ("version", "<u4"), ("header_bytes", "<u4"),
+    ("sb_log2", "<u4"), ("sblocks", "<u4"), ("pages", "<u4"), ("ring", "<u4"),
+    ("nclasses", "<u4"), ("cls_lines", "<u4"), ("flist_words", "<u4"), ("err", "<u4"),
+    ("free_head", "<u8"), ("free_tail", "<u8"), ("ring_avail", "<u4"), ("reserved", "<u4"),
+    ("cls_shards", "<u4", (16,)),
+    ("off_cls", "<u8"), ("off_state", "<u8"), ("off_home", "<u8"), ("off_flist", "<u8"),
+    ("off_region", "<u8"), ("total_bytes", "<u8")])
+assert IMAGE_HEADER.itemsize == 184  # struct kma_image_header (kma.h)
+
+
+def image_header(buf: np.ndarray) -> dict:
+    """The header of a heap image (kma_image_save) as a dict."""
+    buf = np.asarray(buf, np.uint8).reshape(-1)
+    if buf.nbytes < IMAGE_HEADER.itemsize:
+        raise ValueError("not a heap image: shorter than its header")
+    h = buf[:IMAGE_HEADER.itemsize].view(IMAGE_HEADER)[0]
+    if bytes(h["magic"]) != IMAGE_MAGIC:
+        raise ValueError("not a heap image: bad magic")
+    d = {k: (h[k].tolist() if k == "cls_shards" else (bytes(h[k]) if k == "magic" else int(h[k])))
+         for k in IMAGE_HEADER.names}
+    if d["total_bytes"] > buf.nbytes:
+        raise ValueError("heap image truncated")
+    return d
+
+
+def image_from_bytes(buf: np.ndarray, cls_size: list, cls_slots: list, region: bool = True) -> HeapImage:
+    """Decode a saved heap image into the HeapImage the checkers take (the
+    same content kma_snapshot reports).  cls_size / cls_slots are the size
+    tables of the image's superblock size (Heap.cls_size / cls_slots)."""
+    buf = np.asarray(buf, np.uint8).reshape(-1)
+    h = image_header(buf)
+    nsb, nw = h["sblocks"], h["flist_words"]
+    cls = buf[h["off_cls"]:h["off_cls"] + 4 * h["cls_lines"]].view("<u4").copy()
+    state = buf[h["off_state"]:h["off_state"] + 4 * nsb].view("<u4").copy()
+    words = buf[h["off_flist"]:h["off_flist"] + 8 * nw].view("<u8")
+    fl: list | None = []
+    if h["ring"]:
+        hd, tl = h["free_head"], h["free_tail"]
+        if tl - hd > nsb:
+            fl = None
+        else:
+            fl = [int(words[p % nw]) & 0xFFFFFFFF for p in range(hd, tl)]
+    else:
+        idx = h["free_head"] & 0xFFFFFFFF
+        while idx != 0:
+            if len(fl) >= nsb or idx > nw:
+                fl = None
+                break
+            fl.append(idx - 1)
+            idx = int(words[idx - 1]) & 0xFFFFFFFF
+    reg = None
+    if region:
+        reg = buf[h["off_region"]:h["off_region"] + (nsb << h["sb_log2"])].copy()
+    nc = h["nclasses"]
+    return HeapImage(sb_size_log2=h["sb_log2"], sblocks=nsb, pages=h["pages"], nclasses=nc,
+                     cls_size=list(cls_size)[:nc], cls_slots=list(cls_slots)[:nc], cls_raw=cls,
+                     cls_shards=h["cls_shards"][:nc], state=state,
+                     freelist=None if fl is None else np.asarray(fl, np.int64), region=reg)
+
+
 def mask_headers(region: np.ndarray, sb_size_log2: int) -> np.ndarray:
     """Zero the first 12 bytes of every superblock (a copy)."""
     r = np.array(region, dtype=np.uint8, copy=True).reshape(-1, 1 << sb_size_log2)

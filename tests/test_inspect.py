@@ -80,3 +80,65 @@ def test_canonical_empty_after_drain_and_not_before():
         out = p.replay(full)
         img, _ = image_from_port(p, 40, 12, full, out)
         assert ins.check_canonical_empty(img) == []
+
+
+def encode_image(img, ring):
+    """A heap image (the kma_image_save layout) of an oracle-built state,
+    with the free list as ring slots or as Michael-Scott queue links."""
+    al = lambda x: (x + 255) & ~255
+    nsb = img.sblocks
+    nw = img.pages if ring else nsb
+    h = np.zeros(1, ins.IMAGE_HEADER)
+    h["magic"], h["version"], h["header_bytes"] = ins.IMAGE_MAGIC, 1, ins.IMAGE_HEADER.itemsize
+    h["sb_log2"], h["sblocks"], h["pages"], h["ring"] = img.sb_size_log2, nsb, img.pages, int(ring)
+    h["nclasses"], h["cls_lines"], h["flist_words"] = img.nclasses, len(img.cls_raw), nw
+    shards = np.zeros(16, np.uint32)
+    shards[:img.nclasses] = img.cls_shards
+    h["cls_shards"] = shards
+    fl = np.zeros(nw, np.uint64)
+    order = [int(x) for x in img.freelist]
+    if ring:
+        head = 5  # tickets need not start at 0: slots are taken modulo the ring size
+        for k, s in enumerate(order):
+            p = head + k
+            fl[p % nw] = ((p + 1) << 32) | s
+        h["free_head"], h["free_tail"] = head, head + len(order)
+    else:
+        for a, b in zip(order, order[1:]):
+            fl[a] = (7 << 32) | (b + 1)
+        h["free_head"], h["free_tail"] = (3 << 32) | (order[0] + 1), (9 << 32) | (order[-1] + 1)
+    o = al(ins.IMAGE_HEADER.itemsize)
+    h["off_cls"] = o; o = al(o + 4 * len(img.cls_raw))
+    h["off_state"] = o; o = al(o + 4 * nsb)
+    h["off_home"] = o; o = al(o + 2 * nsb)
+    h["off_flist"] = o; o = al(o + 8 * nw)
+    h["off_region"] = o; o += len(img.region)
+    h["total_bytes"] = o
+    buf = np.zeros(o, np.uint8)
+    buf[:ins.IMAGE_HEADER.itemsize] = h.view(np.uint8)
+    put = lambda off, a: buf.__setitem__(slice(off, off + a.nbytes), a.view(np.uint8))
+    put(int(h["off_cls"][0]), np.asarray(img.cls_raw, "<u4"))
+    put(int(h["off_state"][0]), np.asarray(img.state, "<u4"))
+    put(int(h["off_flist"][0]), fl.astype("<u8"))
+    put(int(h["off_region"][0]), np.asarray(img.region, np.uint8))
+    return buf
+
+
+def test_image_bytes_decode_to_the_oracle_state():
+    ops = make_stream(9, 900, 12)
+    with oracle.Port(48, 12) as p:
+        out = p.replay(ops)
+        img, _ = image_from_port(p, 48, 12, ops, out)
+    want = ins.decode(img)
+    for ring in (True, False):
+        buf = encode_image(img, ring)
+        got = ins.decode(ins.image_from_bytes(buf, img.cls_size, img.cls_slots))
+        for f in ("cls", "sb_size", "sb_slots", "sb_free", "freelist", "region"):
+            assert np.array_equal(getattr(want, f), getattr(got, f)), (ring, f)
+    import pytest
+    with pytest.raises(ValueError):
+        ins.image_header(buf[:-1])
+    bad = buf.copy()
+    bad[0] ^= 1
+    with pytest.raises(ValueError):
+        ins.image_header(bad)
