@@ -265,6 +265,58 @@ def measure_forms(quick: bool = False) -> dict:
     out["served_c5"] = {"heap_bytes": 64 << 30, "slots": 16, "occupancy_limit": 0.85,
                         "graph": "N log-uniform 1k..4M vertices, degrees ~ d^-2.1 on 1..4096",
                         "heap_error_flags": flags, "loads": served}
+    out["graph_build"] = measure_graph_build(quick)
+    return out
+
+
+def edge_mix(a, b):
+    """mix(source, sink) as the library computes it (SplitMix64 finaliser
+    of source << 32 | sink), vectorised."""
+    import numpy as np
+    with np.errstate(over="ignore"):
+        z = (a.astype(np.uint64) << np.uint64(32) | b.astype(np.uint64)) + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def measure_graph_build(quick: bool = False) -> dict:
+    """The tree driver's graph build (nodes in a clTree, a clQueue of links
+    per node, every node and link a heap block) on synthetic edges: each
+    build is followed by the teardown that frees every block, and must give
+    the edge multiset back and leave the heap canonically empty.  Two rank
+    distributions: Zipf(1.1), where the hottest vertex's one link queue
+    takes a large share of all enqueues (it bounds the build: enqueues on
+    one queue serialise), and uniform."""
+    import statistics
+    import numpy as np
+    from kma_b200 import Heap, graph
+    from kma_b200 import inspect as ins
+    n_e, n_v = (1 << 22, 1 << 20) if not quick else (1 << 18, 1 << 16)
+    threads = 148 * 1024
+    out = {"edges": n_e, "vertices_drawn_from": n_v, "threads": threads, "heap_bytes": 1 << 30,
+           "sb_size": 1 << 14, "keys": "distinct random u32 per vertex rank"}
+    for name, skew in (("zipf1.1", 1.1), ("uniform", 0.0)):
+        e = graph.synth_edges(0x6A, n_e, n_v, skew=skew)
+        m = edge_mix(e[:, 0], e[:, 1])
+        want = dict(nodes=len(np.unique(e)), links=n_e, edge_xor=int(np.bitwise_xor.reduce(m)),
+                    edge_sum=int(m.sum(dtype=np.uint64)))
+        max_out = int(np.unique(e[:, 0], return_counts=True)[1].max())
+        ms, ok, lost = [], True, 0
+        with Heap((1 << 30) >> 14, 14) as h:
+            for _ in range(3):
+                st, _ = graph.build(h, e, threads=threads, free_after=True)
+                ms.append(float(st["build_ms"]))
+                lost = int(st["lost_adds"])
+                ok = ok and all(int(st[k]) == v for k, v in want.items()) and \
+                    st["err"] == 0 and st["nulls"] == 0 and st["sorted"] == 1
+            empty = ins.check_canonical_empty(h.snapshot(), h.bitmaps()) == []
+            flags = h.error_flags()
+        t = statistics.median(ms)
+        out[name] = {"nodes": want["nodes"], "max_out_degree": max_out, "build_ms": round(t, 3),
+                     "medges_per_s": round(n_e / t / 1e3, 2), "lost_adds": lost,
+                     "edges_conserved": bool(ok), "empty_after_teardown": bool(empty),
+                     "heap_error_flags": flags}
     return out
 
 

@@ -168,12 +168,29 @@ struct clq_link_aligned {
 	static __device__ __forceinline__ bool ok(unsigned long long) { return true; }
 };
 
+#ifndef KMA_CONTEND_MAX_NS
+#define KMA_CONTEND_MAX_NS 4096u
+#endif
+/* After a CAS lost to another thread on a contended word: a randomised
+ * exponential wait (__nanosleep(t) sleeps somewhere in [0, 2t]), 64 ns
+ * doubling per consecutive loss up to KMA_CONTEND_MAX_NS.  Retrying at
+ * once floods the word's L2 slice with requests that queue ahead of the
+ * winner's next step; spread out, the retries let one thread through per
+ * round trip. */
+__device__ __forceinline__ void contend(uint32_t &losses)
+{
+	uint32_t t = 64u << (losses < 10 ? losses : 10);
+	__nanosleep(t < KMA_CONTEND_MAX_NS ? t : KMA_CONTEND_MAX_NS);
+	losses++;
+}
+
 template <class L>
 __device__ inline int clq_enqueue(kma_clqueue *q, unsigned long long it_p, uint32_t *err, uint32_t spin_limit)
 {
 	if (it_p == 0 || it_p == KMA_Q_POISON || (it_p & ~KMA_PTR_MASK) || !L::ok(it_p))
 		return 0;
 	st_release64(L::at(it_p), 0ull);
+	uint32_t losses = 0;
 	for (uint32_t it = 0; it < spin_limit; it++) {
 		unsigned long long t = ld_acquire64(&q->tail);
 		if (qp_ptr(t) == 0) {
@@ -193,6 +210,7 @@ __device__ inline int clq_enqueue(kma_clqueue *q, unsigned long long it_p, uint3
 				cas64_acqrel(&q->tail, t, qp_next(t, it_p));
 				return 1;
 			}
+			contend(losses);
 		} else if (n == KMA_Q_POISON) {
 			/* the tail item is being dequeued: it either goes (the
 			 * queue empties) or its link comes back */
