@@ -113,6 +113,22 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The largest x over all ranks: a replicated job takes as long as its
+    slowest replica.  Every rank must call it (a collective when world > 1)."""
+    if world == 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, ops_per_rank_step: int, steps: int, total_ms: float) -> float:
+    """Whole-job M ops/s: every rank's ops over the slowest rank's time."""
+    return world * ops_per_rank_step * steps / (total_ms / 1e3) / 1e6
+
+
 # ---------------------------------------------------------------- CPU legs
 def cpu_run(kind_pref: str, items: int, threads: int, timeout: float) -> dict:
     """Run the reference's kma.cl (oracle/_ref; the C restatement when the
@@ -403,12 +419,31 @@ def run_ours(args) -> int:
         heap.close()
         return 0
     ops_step = st["mallocs"] + st["frees"]
-    total_ms = sum(step_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    total_ms = max_over_ranks(sum(step_ms), world)
+    value = job_rate(world, ops_step, args.steps, total_ms)
+
+    # end to end through the host-buffer C ABI call, on every rank (pinned seeds in,
+    # per-item hashes + counters out)
+    g = np.arange(ITEMS, dtype=np.uint64)
+    seeds_np = np.uint64(SEED) ^ (g * np.uint64(0x9E3779B97F4A7C15))
+    seeds = torch.from_numpy(seeds_np.view(np.int64)).pin_memory()
+    hashes = torch.empty(ITEMS, dtype=torch.int64).pin_memory()
+    wl.run_host(seeds.data_ptr(), ROUNDS, mode, hashes.data_ptr(), stream)
+    torch.cuda.synchronize()
     if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_ms = float(t.item())
-    value = world * ops_step * args.steps / (total_ms / 1e3) / 1e6
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        st_e = wl.run_host(seeds.data_ptr(), ROUNDS, mode, hashes.data_ptr(), stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world) / args.steps
+    e2e = {"value": round(job_rate(world, st_e["mallocs"] + st_e["frees"], 1, e2e_ms), 3),
+           "unit": UNIT, "h2d_bytes_per_step": ITEMS * 8,
+           "d2h_bytes_per_step": ITEMS * 8 + 56,
+           "ms_per_step": round(e2e_ms, 3),
+           "call": "kma_wl_run_host (host seeds in, host hashes + counters out)"}
 
     out = None
     if rank == 0:
@@ -471,26 +506,6 @@ def run_ours(args) -> int:
             st_p = wl.stats(stream)
             plain_default = (st_p["mallocs"] + st_p["frees"]) / (statistics.mean(p_ms) / 1e3) / 1e6
 
-        # end to end through the host-buffer C ABI call (pinned seeds in,
-        # per-item hashes + counters out)
-        g = np.arange(ITEMS, dtype=np.uint64)
-        seeds_np = np.uint64(SEED) ^ (g * np.uint64(0x9E3779B97F4A7C15))
-        seeds = torch.from_numpy(seeds_np.view(np.int64)).pin_memory()
-        hashes = torch.empty(ITEMS, dtype=torch.int64).pin_memory()
-        wl.run_host(seeds.data_ptr(), ROUNDS, mode, hashes.data_ptr(), stream)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            st_e = wl.run_host(seeds.data_ptr(), ROUNDS, mode, hashes.data_ptr(), stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms = e0.elapsed_time(e1) / args.steps
-        e2e = {"value": round((st_e["mallocs"] + st_e["frees"]) / (e2e_ms / 1e3) / 1e6, 3),
-               "unit": UNIT, "h2d_bytes_per_step": ITEMS * 8,
-               "d2h_bytes_per_step": ITEMS * 8 + 56,
-               "ms_per_step": round(e2e_ms, 3),
-               "call": "kma_wl_run_host (host seeds in, host hashes + counters out)"}
 
         cpu = None
         if not args.no_cpu_baseline:
