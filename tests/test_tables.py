@@ -20,7 +20,7 @@ def expand(trans, sb):
     return out
 
 
-def test_golden_matches_survey_values():
+def test_golden_matches_reference_known_values():
     # the values the reference produces, kma.cl:55-113 at 4 KiB
     g = GOLDEN["12"]
     assert g["size_by_sbid"] == [4, 8, 16, 32, 64, 124, 252, 508, 1020, 2040, 4080]
