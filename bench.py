@@ -336,6 +336,33 @@ def measure_graph_build(quick: bool = False) -> dict:
     return out
 
 
+def measure_cpu_baseline() -> dict:
+    """The reference's kma.cl as host C on this host's cores: a quarter of
+    the work-items on all hardware threads (the reported baseline), and an
+    eighth of them on one thread (the reference's CPU throughput falls as
+    threads are added, so both are given)."""
+    threads = os.cpu_count() or 1
+    items = ITEMS // 4
+    c = cpu_run("reference", items, threads, timeout=120)
+    if "error" in c:
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"unavailable: {c['error']}"}
+    cpu = {"value": round((c["mallocs"] + c["frees"]) / c["seconds"] / 1e6, 3),
+           "unit": UNIT, "cores": threads, "kind": c["kind"],
+           "sample": f"{items} of {ITEMS} work-items x {ROUNDS} rounds, round-robin on "
+                     f"{threads} pthreads (the reference's kma.cl as host C); "
+                     f"its own tag faults: {c['bad_tags']}"}
+    items1 = ITEMS // 8
+    c1 = cpu_run("reference", items1, 1, timeout=120)
+    if "error" not in c1:
+        cpu["one_thread"] = {"value": round((c1["mallocs"] + c1["frees"]) / c1["seconds"] / 1e6, 3),
+                             "unit": UNIT, "sample": f"{items1} of {ITEMS} work-items x {ROUNDS} rounds "
+                                                     f"on 1 thread; its own tag faults: {c1['bad_tags']}"}
+    else:
+        cpu["one_thread"] = {"value": None, "unit": UNIT, "sample": f"unavailable: {c1['error']}"}
+    return cpu
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args) -> int:
     import numpy as np
@@ -507,20 +534,7 @@ def run_ours(args) -> int:
             plain_default = (st_p["mallocs"] + st_p["frees"]) / (statistics.mean(p_ms) / 1e3) / 1e6
 
 
-        cpu = None
-        if not args.no_cpu_baseline:
-            threads = os.cpu_count() or 1
-            items = ITEMS // 4
-            c = cpu_run("reference", items, threads, timeout=120)
-            if "error" not in c:
-                cpu = {"value": round((c["mallocs"] + c["frees"]) / c["seconds"] / 1e6, 3),
-                       "unit": UNIT, "cores": threads, "kind": c["kind"],
-                       "sample": f"{items} of {ITEMS} work-items x {ROUNDS} rounds, round-robin on "
-                                 f"{threads} pthreads (the reference's kma.cl as host C); "
-                                 f"its own tag faults: {c['bad_tags']}"}
-            else:
-                cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
-                       "sample": f"unavailable: {c['error']}"}
+        cpu = None if args.no_cpu_baseline else measure_cpu_baseline()
 
         out = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
