@@ -155,16 +155,26 @@ print(json.dumps(st))
         return {"error": f"timed out after {timeout:.0f} s"}
 
 
+def cpu_sample(items: int, threads: int, kind: str) -> str:
+    what = ("kma.cl+clIndexedQueue.cl built unmodified as host C" if kind == "reference"
+            else "C restatement of kma.cl")
+    return (f"{items} of the {ITEMS} work-items x {ROUNDS} rounds per step (1 GiB heap, 16 KiB "
+            f"superblocks), work-items round-robin on {threads} pthread{'s' if threads != 1 else ''}, "
+            f"each to completion; {what}")
+
+
 def run_reference(args) -> int:
+    """The reference arm: the reference's own kma.cl as host C on all host
+    threads, every step the whole config-2 program (all work-items)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    items = ITEMS // 4
+    items = ITEMS
     vals = []
     last = None
     for k in range(args.warmup + args.steps):
-        st = cpu_run("reference", items, threads, timeout=120)
+        st = cpu_run("reference", items, threads, timeout=300)
         if "error" in st:
             print(json.dumps({"impl": "reference", "unavailable": f"CPU run failed: {st['error']}"}))
             return 0
@@ -173,18 +183,16 @@ def run_reference(args) -> int:
             last = st
     v = statistics.median(vals)
     kind = last["kind"]
-    sample = (f"{items} of the {ITEMS} work-items x {ROUNDS} rounds per step (1 GiB heap, 16 KiB "
-              f"superblocks), work-items round-robin on {threads} pthreads, each to completion; "
-              f"{'kma.cl+clIndexedQueue.cl built unmodified as host C' if kind == 'reference' else 'C restatement of kma.cl'}")
     line = {"metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * last["seconds"], 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "items_per_step": items, "rounds": ROUNDS,
+            "config": {"workload": WORKLOAD, "items": items, "rounds": ROUNDS,
                        "heap_bytes": SBLOCKS << SB_LOG2, "sb_size": 1 << SB_LOG2,
+                       "ops_per_step": int(last["mallocs"] + last["frees"]), "threads": threads,
                        "invariant_faults": int(last["bad_tags"]), "nulls": int(last["nulls"])},
             "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": sample},
+                             "sample": cpu_sample(items, threads, kind)},
             "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -336,30 +344,28 @@ def measure_graph_build(quick: bool = False) -> dict:
     return out
 
 
-def measure_cpu_baseline() -> dict:
-    """The reference's kma.cl as host C on this host's cores: a quarter of
-    the work-items on all hardware threads (the reported baseline), and an
-    eighth of them on one thread (the reference's CPU throughput falls as
-    threads are added, so both are given)."""
+def measure_cpu_baseline(items: int | None = None) -> dict:
+    """The reference's kma.cl as host C on this host's cores, over the same
+    sample on all hardware threads (the reported baseline) and on one
+    thread (the reference's CPU throughput falls as threads are added, so
+    both are given).  The sample is the whole config-2 program unless
+    `items` names fewer work-items."""
     threads = os.cpu_count() or 1
-    items = ITEMS // 4
-    c = cpu_run("reference", items, threads, timeout=120)
+    items = ITEMS if items is None else items
+    c = cpu_run("reference", items, threads, timeout=300)
     if "error" in c:
         return {"value": None, "unit": UNIT, "cores": threads, "kind": "reference",
                 "sample": f"unavailable: {c['error']}"}
     cpu = {"value": round((c["mallocs"] + c["frees"]) / c["seconds"] / 1e6, 3),
            "unit": UNIT, "cores": threads, "kind": c["kind"],
-           "sample": f"{items} of {ITEMS} work-items x {ROUNDS} rounds, round-robin on "
-                     f"{threads} pthreads (the reference's kma.cl as host C); "
-                     f"its own tag faults: {c['bad_tags']}"}
-    items1 = ITEMS // 8
-    c1 = cpu_run("reference", items1, 1, timeout=120)
+           "sample": cpu_sample(items, threads, c["kind"]) + f"; its own tag faults: {c['bad_tags']}"}
+    c1 = cpu_run("reference", items, 1, timeout=300)
     if "error" not in c1:
         cpu["one_thread"] = {"value": round((c1["mallocs"] + c1["frees"]) / c1["seconds"] / 1e6, 3),
-                             "unit": UNIT, "sample": f"{items1} of {ITEMS} work-items x {ROUNDS} rounds "
-                                                     f"on 1 thread; its own tag faults: {c1['bad_tags']}"}
+                             "unit": UNIT, "cores": 1,
+                             "sample": cpu_sample(items, 1, c1["kind"]) + f"; its own tag faults: {c1['bad_tags']}"}
     else:
-        cpu["one_thread"] = {"value": None, "unit": UNIT, "sample": f"unavailable: {c1['error']}"}
+        cpu["one_thread"] = {"value": None, "unit": UNIT, "cores": 1, "sample": f"unavailable: {c1['error']}"}
     return cpu
 
 

@@ -598,22 +598,57 @@ bool kma_image_valid(const kma_heap &hh, const kma_image_header &hdr, const uint
 		if (c >= hh.nclasses || slots != hh.cls_slots[c] || fr > slots || home[s] >= hh.cls_nsh[c])
 			return false;
 	}
+	/* The free list must be one a quiescent heap can hold: every queued
+	 * superblock once (a second entry would be handed out twice), each
+	 * with free count 0 (detaching for the free list zeroes it; a live
+	 * superblock on the list would be reformatted under its blocks). */
+	std::vector<unsigned char> queued(nsb, 0);
+	auto take = [&](uint32_t s) {
+		if (s >= nsb || queued[s] || (state[s] & KMA_ST_FREE_MASK) != 0)
+			return false;
+		queued[s] = 1;
+		return true;
+	};
 	if (hdr.ring) {
-		if (hdr.free_tail < hdr.free_head || hdr.free_tail - hdr.free_head > hh.ring_cap)
+		const uint64_t head = hdr.free_head, tail = hdr.free_tail, cap = hh.ring_cap;
+		if (tail < head || tail - head > cap || hdr.flist_words != cap)
 			return false;
-		int32_t avail = (int32_t)hdr.ring_avail;
-		if (avail > (int32_t)hh.ring_cap || avail < -(int32_t)hh.ring_cap)
+		/* completed enqueues not yet claimed: the queued count exactly */
+		if ((int64_t)(int32_t)hdr.ring_avail != (int64_t)(tail - head))
 			return false;
-		for (uint32_t i = 0; i < hdr.flist_words; i++)
-			if ((uint32_t)fl[i] >= nsb)
+		/* slot of ticket p: {seq p+1 | sb} when filled (head <= p < tail),
+		 * {seq p | -} when free for the enqueue with ticket p */
+		for (uint64_t p = head; p < head + cap; p++) {
+			const unsigned long long w = fl[p % cap];
+			const uint32_t seq = (uint32_t)(w >> 32);
+			if (p < tail) {
+				if (seq != (uint32_t)(p + 1) || !take((uint32_t)w))
+					return false;
+			} else if (seq != (uint32_t)p) {
 				return false;
+			}
+		}
 	} else {
+		/* MS queue over superblock indices (idx = s + 1): the chain from
+		 * the head (the dummy) must end at the tail with a null link, with
+		 * no superblock twice (a cycle never ends) */
 		uint32_t hi = (uint32_t)hdr.free_head, ti = (uint32_t)hdr.free_tail;
 		if (hi == 0 || hi > nsb || ti == 0 || ti > nsb)
 			return false;
 		for (uint32_t i = 0; i < hdr.flist_words; i++)
 			if ((uint32_t)fl[i] > nsb)
 				return false;
+		uint32_t idx = hi;
+		for (;;) {
+			if (!take(idx - 1))
+				return false;
+			uint32_t nx = (uint32_t)fl[idx - 1];
+			if (nx == 0)
+				break;
+			idx = nx;
+		}
+		if (idx != ti)
+			return false;
 	}
 	return true;
 }

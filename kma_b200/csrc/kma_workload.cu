@@ -27,6 +27,10 @@
 #include "kma_wl_common.cuh"
 
 #define WL_CAP 32
+/* Counter words behind wl_dev.stats: [0..5] kma_wl_stats counters, [8] the
+ * hash XOR of kma_wl_stats_get, [10..13] phase cycles, [16..23] tallies.
+ * Every scratch layout reserves this many. */
+#define WL_STATS_WORDS 32
 
 struct wl_dev {
 	uint64_t items;
@@ -416,7 +420,7 @@ __global__ void k_wl_begin(wl_dev w, uint64_t seed, const uint64_t *seeds)
 	if (g == 0) {
 		for (int i = 0; i < 6; i++)
 			w.stats[i] = 0;
-		for (int i = 10; i < 24; i++)
+		for (int i = 10; i < WL_STATS_WORDS; i++)
 			w.stats[i] = 0;
 	}
 	for (; g < w.items; g += (uint64_t)gridDim.x * blockDim.x) {
@@ -487,7 +491,7 @@ extern "C" int kma_wl_create(kma_heap_t h, int program, uint64_t items, kma_wl_t
 	size_t off_loff = (off_nlive + 4 * n + 255) & ~(size_t)255;
 	size_t off_lsize = off_loff + 8 * n * WL_CAP;
 	size_t off_stats = (off_lsize + 4 * n * WL_CAP + 255) & ~(size_t)255;
-	size_t off_seeds = off_stats + 256;
+	size_t off_seeds = off_stats + 8 * WL_STATS_WORDS;
 	size_t total = off_seeds + 8 * n;
 	if (cudaMalloc(&w->scratch, total) != cudaSuccess) {
 		cudaGetLastError();
@@ -815,7 +819,7 @@ extern "C" int kma_wl_run_noalloc(kma_heap_t h, int program, uint64_t items, con
 	size_t o_loff = up256(o_nlive + 4 * n);
 	size_t o_lsize = up256(o_loff + 8 * n * WL_CAP);
 	size_t o_stats = up256(o_lsize + 4 * n * WL_CAP);
-	if (o_stats + 64 > sizeof(kma_noalloc_scratch))
+	if (o_stats + 8 * WL_STATS_WORDS > sizeof(kma_noalloc_scratch))
 		return KMA_EINVAL;
 	wl_dev d;
 	d.items = items;

@@ -113,3 +113,68 @@ def test_damaged_image_is_refused_and_heap_unchanged():
         # the untouched image still loads
         b.image_load(img)
         assert_same_state(full_state(a), full_state(b))
+
+
+def _header_view(buf):
+    return buf[:ins.IMAGE_HEADER.itemsize].view(ins.IMAGE_HEADER)
+
+
+def test_inconsistent_ring_free_list_is_refused():
+    """A ring free list that a quiescent heap cannot hold: a superblock
+    queued twice, a slot sequence number off its ticket, an availability
+    count that is not the queued count, a queued superblock with free
+    slots.  Each would hand out blocks twice or leave waits to run out."""
+    with Heap(64, 12) as a, Heap(64, 12) as b:
+        a.replay(make_stream(76, 600, 12), MODE_WARP)
+        img = a.image_save()
+        h = ins.image_header(img)
+        assert h["ring"] == 1 and h["free_tail"] - h["free_head"] >= 2
+        cap, hd = h["flist_words"], h["free_head"]
+        fl = lambda buf: buf[h["off_flist"]:h["off_flist"] + 8 * cap].view("<u8")
+        st = lambda buf: buf[h["off_state"]:h["off_state"] + 4 * h["sblocks"]].view("<u4")
+        before = full_state(b)
+
+        def refused(buf):
+            with pytest.raises(KmaError) as e:
+                b.image_load(buf)
+            assert e.value.code == EINVAL
+            assert_same_state(before, full_state(b))
+
+        s0 = int(fl(img)[hd % cap]) & 0xFFFFFFFF
+        bad = img.copy(); w = int(fl(bad)[(hd + 1) % cap])
+        fl(bad)[(hd + 1) % cap] = (w & ~0xFFFFFFFF) | s0; refused(bad)       # queued twice
+        bad = img.copy(); fl(bad)[hd % cap] = int(fl(bad)[hd % cap]) + (1 << 32)
+        refused(bad)                                                         # seq off its ticket
+        bad = img.copy(); _header_view(bad)["ring_avail"] += 1; refused(bad)  # count off
+        bad = img.copy(); st(bad)[s0] = (0 << 28) | (a.cls_slots[0] << 14) | 1
+        refused(bad)                                                         # queued with free slots
+        b.image_load(img)
+        assert_same_state(full_state(a), full_state(b))
+
+
+def test_inconsistent_queue_free_list_is_refused():
+    """The compat heap's MS-queue free list: a chain with a cycle, and a
+    chain that does not end at the tail, are refused."""
+    with Heap(64, 12, compat=True) as a, Heap(64, 12, compat=True) as b:
+        a.replay(make_stream(77, 600, 12), MODE_PLAIN)
+        img = a.image_save()
+        h = ins.image_header(img)
+        nw = h["flist_words"]
+        fl = lambda buf: buf[h["off_flist"]:h["off_flist"] + 8 * nw].view("<u8")
+        hi, ti = h["free_head"] & 0xFFFFFFFF, h["free_tail"] & 0xFFFFFFFF
+        assert hi != ti
+        before = full_state(b)
+
+        def refused(buf):
+            with pytest.raises(KmaError) as e:
+                b.image_load(buf)
+            assert e.value.code == EINVAL
+            assert_same_state(before, full_state(b))
+
+        bad = img.copy(); fl(bad)[ti - 1] = (int(fl(bad)[ti - 1]) & ~0xFFFFFFFF) | hi
+        refused(bad)                                                         # tail links to head
+        bad = img.copy(); hv = _header_view(bad)
+        hv["free_tail"] = (int(hv["free_tail"][0]) & ~0xFFFFFFFF) | hi
+        refused(bad)                                                         # chain ends past the tail
+        b.image_load(img)
+        assert_same_state(full_state(a), full_state(b))
