@@ -1,0 +1,233 @@
+/*
+ * kma_queue_algo.h -- the algorithms of the two lock-free FIFOs
+ * (kma_clqueue, clQueue.cl:27-118; kma_iqueue, clIndexedQueue.cl:44-290),
+ * written once over an atomics policy so that the same text runs on the
+ * GPU (kma_structs.cuh binds gpu-scope PTX atomics) and on host threads
+ * (oracle/queue_harness.cpp binds GCC atomics), where its concurrency
+ * properties are checked before any GPU run.
+ *
+ * Both queues append with an EXCHANGE on the tail, never a CAS loop:
+ *
+ *   prev = exchange(tail, last item of the new chain); link prev to the chain
+ *
+ * so an append of one item or of a whole chain (a warp's items, linked
+ * in lane order beforehand) costs one atomic on the shared tail word and
+ * always succeeds, and the tail moves straight to the chain's last item.
+ * There is no lagging tail for later appends to help forward one link at
+ * a time: the Michael-Scott queue of the reference moves the tail with a
+ * second CAS after linking, and a chain appended that way leaves the tail
+ * on the chain's FIRST item, so every later enqueue first walks it along.
+ * Between the exchange and the link the chain is not yet reachable from
+ * the head; a dequeuer that meets the end of the linked part meanwhile
+ * sees the queue as ending there (the pointer queue waits a bounded time
+ * when that end is its last item), the one window in which these queues
+ * are not linearizable.  Serially (one operation at a time) both behave
+ * exactly as the reference's queues: same results, same head, tail and
+ * links.
+ *
+ * Policy `O` provides, on 64-bit words:
+ *   ld(p)        acquire load        st(p, v)     release store
+ *   ld_rlx(p)    relaxed load        st_rlx(p, v) relaxed store
+ *   xchg(p, v)   acq_rel exchange    cas(p, c, v) acq_rel compare-and-swap, returns the old value
+ *   pause(it)    back-off after `it` fruitless tries
+ * Every wait is bounded by `limit` tries; expiry returns failure and the
+ * caller records KMA_ERR_TIMEOUT.
+ */
+#ifndef KMA_QUEUE_ALGO_H
+#define KMA_QUEUE_ALGO_H
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define KQ_FN __device__ __forceinline__
+#else
+#define KQ_FN inline
+#endif
+
+namespace kma_q {
+
+typedef unsigned long long u64;
+
+/* ------------------------------------------------------------------ */
+/* pointer queue (clQueue)                                             */
+/* ------------------------------------------------------------------ */
+/* head: {tag:16 | item pointer:48}, the tag bumped by every change, so a
+ * stale CAS on it fails; tail: the last item's pointer (0 = empty),
+ * changed only by exchange (append) and by the dequeue that empties the
+ * queue (CAS last item -> 0).  Item links: next item, 0 = none yet,
+ * POISON = held by a dequeuer or removed (the reference's claim,
+ * clQueue.cl:97; removed items keep it until enqueued again). */
+const u64 POISON = 1ull;
+const int PTR_BITS = 48;
+const u64 PTR_MASK = (1ull << PTR_BITS) - 1ull;
+
+KQ_FN u64 qp_ptr(u64 w) { return w & PTR_MASK; }
+KQ_FN u64 qp_next(u64 w, u64 ptr) { return (((w >> PTR_BITS) + 1ull) << PTR_BITS) | ptr; }
+
+/* Append the chain first..last (its links already set, last's link 0,
+ * all of it written before the call).  1, or 0 when a wait expired. */
+template <class O, class L>
+KQ_FN int clq_append(u64 *headw, u64 *tailw, u64 first, u64 last, uint32_t limit)
+{
+	const u64 prev = O::xchg(tailw, last);
+	if (prev == 0) {
+		/* the queue was empty: the chain becomes the head.  The dequeue
+		 * that emptied the queue may not have cleared the head yet. */
+		for (uint32_t it = 0; it < limit; it++) {
+			const u64 h = O::ld(headw);
+			if (qp_ptr(h) == 0 && O::cas(headw, h, qp_next(h, first)) == h)
+				return 1;
+			O::pause(it);
+		}
+		return 0;
+	}
+	/* link after prev; a dequeuer that holds prev's link (POISON) to see
+	 * whether prev is the last item gives it back at once */
+	u64 *pl = L::at(prev);
+	for (uint32_t it = 0; it < limit; it++) {
+		const u64 old = O::cas(pl, 0ull, first);
+		if (old == 0)
+			return 1;
+		if (old != POISON)
+			return 0; /* prev has a successor already: an item enqueued twice */
+		O::pause(it);
+	}
+	return 0;
+}
+
+/* Take the head item and up to k-1 items after it, in FIFO order, into
+ * out[].  Returns the number taken; 0 when the queue is empty, and 0 with
+ * *timed_out set when a wait expired.  The caller holds nothing after.
+ *
+ * The head item is claimed by exchanging its link for POISON (as the
+ * reference does); while a dequeuer holds it nobody else can move the
+ * head, so the items behind it are read without further atomics and the
+ * head moves past all of them with one store.  Taken items keep POISON
+ * in their links. */
+template <class O, class L>
+KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint32_t limit, bool *timed_out)
+{
+	*timed_out = false;
+	uint32_t it = 0;
+	while (it < limit) {
+		const u64 h = O::ld(headw);
+		const u64 hp = qp_ptr(h);
+		if (hp == 0)
+			return 0;
+		u64 *hl = L::at(hp);
+		const u64 nx = O::xchg(hl, POISON);
+		if (nx == POISON) {
+			/* another dequeuer holds it, or it left the queue already */
+			O::pause(it++);
+			continue;
+		}
+		/* hp's link is ours; hp is the head unless the head moved since
+		 * it was read (hp taken, then enqueued again elsewhere) */
+		if (O::ld(headw) != h) {
+			O::st(hl, nx);
+			O::pause(it++);
+			continue;
+		}
+		if (nx != 0) {
+			out[0] = hp;
+			uint32_t r = 1;
+			u64 cur = nx;
+			while (r < k) {
+				const u64 n2 = O::ld(L::at(cur));
+				if (n2 == 0 || n2 == POISON)
+					break; /* cur is the last linked item: it stays, as the head */
+				O::st_rlx(L::at(cur), POISON);
+				out[r++] = cur;
+				cur = n2;
+			}
+			O::st(headw, qp_next(h, cur));
+			return r;
+		}
+		/* hp is the last linked item: the only item when the tail still
+		 * names it; otherwise an append has exchanged the tail and is
+		 * about to link after hp */
+		if (O::cas(tailw, hp, 0ull) == hp) {
+			O::st(headw, qp_next(h, 0ull));
+			out[0] = hp;
+			return 1;
+		}
+		/* give the link back and wait for the append to land */
+		O::st(hl, 0ull);
+		while (it < limit && O::ld(hl) == 0ull && O::ld(headw) == h)
+			O::pause(it++);
+	}
+	*timed_out = true;
+	return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* indexed queue (clIndexedQueue)                                      */
+/* ------------------------------------------------------------------ */
+/* Words {tag:32 | index:32}, index 0 = none.  The Michael-Scott queue
+ * with a dummy item, as the reference's: head names the dummy, dequeue
+ * moves head to the dummy's successor and returns the OLD dummy, NULL
+ * when the dummy has no successor.  Appends exchange the tail and then
+ * store the link of the previous tail item, which nobody else writes: a
+ * dummy leaves the queue only once its successor is linked, so the
+ * previous tail item is still in the queue when its link is stored.
+ * A link is written only by the append that links after it (0 -> item)
+ * and by its own item's next enqueue (reset to 0). */
+KQ_FN uint32_t tw_idx(u64 w) { return (uint32_t)w; }
+KQ_FN uint32_t tw_tag(u64 w) { return (uint32_t)(w >> 32); }
+KQ_FN u64 tw_make(uint32_t tag, uint32_t idx) { return ((u64)tag << 32) | idx; }
+
+/* Q provides u64 *link(uint32_t idx); every index the queue can hold,
+ * and 0 (a zero word), has one. */
+template <class O, class Q>
+KQ_FN void iq_append(const Q &q, u64 *tailw, uint32_t first, uint32_t last)
+{
+	const u64 prev = O::xchg(tailw, tw_make(0, last));
+	u64 *pl = q.link(tw_idx(prev));
+	O::st(pl, tw_make(tw_tag(O::ld_rlx(pl)) + 1u, first));
+}
+
+/* Set item idx's link (to 0, or to the next item of a chain) before idx
+ * is appended. */
+template <class O, class Q>
+KQ_FN void iq_set_link(const Q &q, uint32_t idx, uint32_t next)
+{
+	u64 *l = q.link(idx);
+	O::st_rlx(l, tw_make(tw_tag(O::ld_rlx(l)) + 1u, next));
+}
+
+/* Dequeue up to k old dummies into out[] (indices, FIFO order).  Returns
+ * the number taken: 0 when the dummy has no successor, or (with
+ * *timed_out) when the CAS kept losing past `limit` tries.  Reads the
+ * chain behind the head first and moves the head past it with one CAS; a
+ * head that moved meanwhile fails the CAS (its tag changed) and the walk
+ * is retried. */
+template <class O, class Q>
+KQ_FN uint32_t iq_dequeue_n(const Q &q, u64 *headw, uint32_t *out, uint32_t k, uint32_t limit, bool *timed_out)
+{
+	*timed_out = false;
+	for (uint32_t it = 0; it < limit; it++) {
+		const u64 hd = O::ld(headw);
+		uint32_t cur = tw_idx(hd), r = 0;
+		while (r < k) {
+			const uint32_t nx = tw_idx(O::ld(q.link(cur)));
+			if (nx == 0)
+				break;
+			out[r++] = cur;
+			cur = nx;
+		}
+		if (r == 0) {
+			if (O::ld(headw) == hd)
+				return 0;
+			continue;
+		}
+		if (O::cas(headw, hd, tw_make(tw_tag(hd) + 1u, cur)) == hd)
+			return r;
+		O::pause(it);
+	}
+	*timed_out = true;
+	return 0;
+}
+
+} /* namespace kma_q */
+
+#endif /* KMA_QUEUE_ALGO_H */

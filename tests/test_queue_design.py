@@ -1,0 +1,105 @@
+"""The queue algorithms of include/kma_queue_algo.h on host threads (no GPU).
+
+oracle/queue_harness runs the same algorithm text the GPU runs, bound to
+host atomics: producers append chains (a warp's items) and single items,
+consumers take batches and re-append some of what they take (items leave
+and re-enter the queue), and an append sometimes sleeps between its
+exchange of the tail and its link -- the window in which its chain is not
+reachable yet.  Every run must conserve every append, keep each appender's
+order, end with a consistent head/tail, and never run out a wait.
+
+The second test plants one mistake at a time in a scratch copy of the
+algorithm (never in the product) and checks the harness reports it, so a
+passing run means something.
+"""
+import json
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE = os.path.join(ROOT, "oracle")
+HARNESS = os.path.join(ORACLE, "queue_harness")
+ALGO = os.path.join(ROOT, "include", "kma_queue_algo.h")
+
+# threads chains max_chain deq_batch delay_prob seed producers recycle
+CONFIGS = [
+    "8 20000 1 1 0.01 1 1 0.5",      # single items, one producer: the queue is mostly empty
+    "8 20000 4 4 0.01 2 2 0.5",
+    "8 5000 32 32 0.02 3 4 0.5",     # warp-sized chains and batches, many delayed appends
+    "8 3000 32 32 0.002 4 4 0.9",
+    "8 40000 32 32 0.0005 5 4 0",    # no recycling: plain producer/consumer
+    "3 20000 8 8 0.01 6 1 0.5",
+]
+
+
+def have_compiler() -> bool:
+    return shutil.which(os.environ.get("CXX", "g++")) is not None
+
+
+def run(binary, kind, cfg, timeout=300):
+    r = subprocess.run([binary, kind, *cfg.split()], capture_output=True, text=True, timeout=timeout)
+    line = r.stdout.strip().splitlines()[-1] if r.stdout.strip() else "{}"
+    return r.returncode, json.loads(line) if line.startswith("{") else {}
+
+
+@pytest.fixture(scope="module")
+def harness():
+    if not have_compiler():
+        pytest.skip("no C++ compiler")
+    subprocess.run(["make", "-s", "-C", ORACLE, "queue_harness"], check=True)
+    return HARNESS
+
+
+@pytest.mark.parametrize("kind", ["clq", "iq"])
+@pytest.mark.parametrize("cfg", CONFIGS)
+def test_queue_algorithm_conserves_and_keeps_order(harness, kind, cfg):
+    rc, st = run(harness, kind, cfg)
+    assert rc == 0 and st.get("ok"), st
+    assert st["taken"] + st["left"] >= st["appended"] > 0
+    assert st["conservation_faults"] == 0 and st["order_faults"] == 0 and st["timeouts"] == 0
+
+
+# Each mutant breaks one step the algorithm depends on.
+MUTANTS = {
+    # link after the previous tail with a plain store: a dequeuer's hold
+    # of that link (POISON) is overwritten, and its restore then cuts the chain
+    "append_link_store": ("clq", "8 20000 1 1 0.01 1 1 0.5",
+                          "const u64 old = O::cas(pl, 0ull, first);",
+                          "const u64 old = 0; O::st(pl, first);"),
+    # no check that the held item is still the head (ABA after recycling)
+    "no_head_recheck": ("clq", "8 20000 4 4 0.01 2 2 0.5",
+                        "\t\tif (O::ld(headw) != h) {\n\t\t\tO::st(hl, nx);",
+                        "\t\tif (false) {\n\t\t\tO::st(hl, nx);"),
+    # take the last linked item without checking the tail: an append in
+    # its window is lost
+    "last_item_no_tail_cas": ("clq", "8 20000 1 1 0.01 1 1 0.5",
+                              "\t\tif (O::cas(tailw, hp, 0ull) == hp) {",
+                              "\t\tif (true) { O::st(tailw, 0ull);"),
+    # move the indexed queue's head with a plain store: two dequeuers take
+    # the same items
+    "iq_head_store": ("iq", "8 20000 4 4 0.01 2 2 0.5",
+                      "\t\tif (O::cas(headw, hd, tw_make(tw_tag(hd) + 1u, cur)) == hd)\n\t\t\treturn r;",
+                      "\t\tO::st(headw, tw_make(tw_tag(hd) + 1u, cur));\n\t\treturn r;"),
+}
+
+
+@pytest.mark.parametrize("name", sorted(MUTANTS))
+def test_harness_detects_planted_mistakes(harness, tmp_path, name):
+    kind, cfg, old, new = MUTANTS[name]
+    src = open(ALGO).read()
+    assert src.count(old) == 1, f"mutation site of {name} not found once"
+    d = tmp_path / name
+    d.mkdir()
+    (d / "kma_queue_algo.h").write_text(src.replace(old, new))
+    binary = str(d / "h")
+    subprocess.run([os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-pthread", f"-I{d}", "-o", binary,
+                    os.path.join(ORACLE, "queue_harness.cpp")], check=True)
+    try:
+        rc, st = run(binary, kind, cfg, timeout=120)
+    except subprocess.TimeoutExpired:
+        return  # a wait that never ends is a detection too
+    assert rc != 0, f"mutant {name} passed unnoticed: {st}"
