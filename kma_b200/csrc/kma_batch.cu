@@ -168,7 +168,7 @@ __device__ __forceinline__ void bt_round(kma_heap *h, const bt_dev &w, const bt_
 			q = bt_block(h, w.off4[e]);
 			qn = bt_bytes(w.meta[e]);
 		}
-		if (coop_verify(mask, lane, q, qn, (uint32_t)o_g))
+		if (coop_verify_blockwise(mask, lane, q, qn, (uint32_t)o_g))
 			ct.bad++;
 		bt_free(h, cc, lane, q, qn, ct);
 		if (q) {
@@ -202,7 +202,7 @@ __device__ __forceinline__ void bt_round(kma_heap *h, const bt_dev &w, const bt_
 			q = bt_block(h, w.off4[g]);
 			qn = bt_bytes(w.meta[g]);
 		}
-		if (coop_verify(mask, lane, q, qn, tag))
+		if (coop_verify_blockwise(mask, lane, q, qn, tag))
 			ct.bad++;
 		bt_free(h, cc, lane, q, qn, ct);
 		if (full) {

@@ -50,10 +50,12 @@ __device__ __forceinline__ void coop_fill(uint32_t mask, uint32_t lane, void *p,
 /* Blocks of at least this many bytes are verified by the whole warp. */
 #define WL_COOP_BYTES 256u
 
-/* This lane's share of verifying block p (nw words) cooperatively: head
- * words up to the 16-byte boundary, 16-byte vectors lane, lane+32, ...,
- * and tail words.  Nonzero if its share differs from the tag. */
-__device__ __forceinline__ uint32_t verify_share(uint32_t lane, const uint32_t *p, uint32_t nw, uint32_t tag)
+/* The share of the r-th of `width` calling lanes in verifying block p (nw
+ * words) cooperatively: head words up to the 16-byte boundary, 16-byte
+ * vectors r, r+width, ..., and tail words.  Nonzero if its share differs
+ * from the tag. */
+__device__ __forceinline__ uint32_t verify_share(uint32_t r, uint32_t width, const uint32_t *p, uint32_t nw,
+		uint32_t tag)
 {
 	uint32_t head = (uint32_t)((16u - ((uintptr_t)p & 15u)) & 15u) >> 2;
 	head = head < nw ? head : nw;
@@ -62,25 +64,122 @@ __device__ __forceinline__ uint32_t verify_share(uint32_t lane, const uint32_t *
 	const uint4 *v = reinterpret_cast<const uint4 *>(p + head);
 	uint32_t bad = 0;
 #pragma unroll 4
-	for (uint32_t k = lane; k < nv; k += 32) {
+	for (uint32_t k = r; k < nv; k += width) {
 		uint4 x = v[k];
 		bad |= (x.x ^ tag) | (x.y ^ tag) | (x.z ^ tag) | (x.w ^ tag);
 	}
-	if (lane < head)
-		bad |= p[lane] ^ tag;
-	if (lane < tail)
-		bad |= p[head + 4 * nv + lane] ^ tag;
+	for (uint32_t i = r; i < head; i += width)
+		bad |= p[i] ^ tag;
+	for (uint32_t i = r; i < tail; i += width)
+		bad |= p[head + 4 * nv + i] ^ tag;
 	return bad;
 }
+
+/* Vectors each lane has in flight per batch of coop_verify_rows (4:
+ * config 2's rounds kernel, 64 registers, measured 8.73 against 8.90 ms
+ * per launch for the block-by-block loop; 6 and 8 spill more and measured
+ * 9.57 and 10.02 ms). */
+#ifndef WL_VERIFY_SLOTS
+#define WL_VERIFY_SLOTS 4
+#endif
+
+/* Verify every lane's block (p may be NULL) against its tag; true in the
+ * owner lane of a block with a word that differs.  Every lane of `mask`
+ * calls it.
+ *
+ * Small blocks: the owner reads its own, 16-byte loads unrolled by eight.
+ * Blocks of WL_COOP_BYTES or more: their 16-byte aligned bodies are cut
+ * into rows of one vector per calling lane, rows of all big blocks laid
+ * end to end in lane order; the r-th calling lane reads vector r of each
+ * row.  A batch is the next
+ * WL_VERIFY_SLOTS rows, whichever blocks they belong to: every lane issues
+ * all the batch's loads before it compares any, so a pass over the warp's
+ * blocks costs one memory round trip per batch rather than one per block
+ * (a loop over blocks consumes each block's loads before it can issue the
+ * next block's).  The row schedule is the same in every lane, so which
+ * block a row belongs to, its base and its tag are broadcast by shuffles;
+ * the owner of a big block reads its head and tail words (the few before
+ * and after the aligned body) along with the small blocks. */
+#if WL_VERIFY_SLOTS > 0
+__device__ __forceinline__ bool coop_verify_rows(uint32_t mask, uint32_t lane, const void *p, uint32_t n,
+		uint32_t tag)
+{
+	const uint32_t *w = (const uint32_t *)p;
+	const bool big = p && n >= WL_COOP_BYTES;
+	const uint32_t nw = p ? n >> 2 : 0u;
+	uint32_t head = (uint32_t)((16u - ((uintptr_t)p & 15u)) & 15u) >> 2;
+	head = head < nw ? head : nw;
+	const uint32_t nv = (nw - head) >> 2;
+	uint32_t bad = 0;
+	if (p) {
+		/* head words, then (small blocks) the body, then tail words */
+		for (uint32_t i = 0; i < head; i++)
+			bad |= w[i] ^ tag;
+		if (!big) {
+			const uint4 *v = reinterpret_cast<const uint4 *>(w + head);
+#pragma unroll 8
+			for (uint32_t k = 0; k < nv; k++) {
+				uint4 x = v[k];
+				bad |= (x.x ^ tag) | (x.y ^ tag) | (x.z ^ tag) | (x.w ^ tag);
+			}
+		}
+		for (uint32_t i = head + 4 * nv; i < nw; i++)
+			bad |= w[i] ^ tag;
+	}
+	uint32_t mb = __ballot_sync(mask, big);
+	uint32_t badbits = 0;
+	const uint32_t width = __popc(mask), rank = __popc(mask & ((1u << lane) - 1u));
+	/* the block whose rows are being scheduled (warp-uniform) */
+	const uint4 *cb = nullptr;
+	uint32_t cj = 0, cnv = 0, crow = 0, crows = 0;
+	while (mb || crow < crows) {
+		uint4 x[WL_VERIFY_SLOTS];
+		uint32_t sj[WL_VERIFY_SLOTS];
+		uint32_t valid = 0;
+#pragma unroll
+		for (int s = 0; s < WL_VERIFY_SLOTS; s++) {
+			if (crow >= crows && mb) {
+				cj = __ffs(mb) - 1;
+				mb &= mb - 1;
+				const uint32_t *pj = (const uint32_t *)__shfl_sync(mask, (unsigned long long)w, cj);
+				cnv = __shfl_sync(mask, nv, cj);
+				const uint32_t hj = __shfl_sync(mask, head, cj);
+				cb = reinterpret_cast<const uint4 *>(pj + hj);
+				crow = 0;
+				crows = (cnv + width - 1) / width;
+			}
+			sj[s] = cj;
+			x[s] = make_uint4(0, 0, 0, 0);
+			if (crow < crows) {
+				const uint32_t k = crow * width + rank;
+				if (k < cnv) {
+					x[s] = cb[k];
+					valid |= 1u << s;
+				}
+				crow++;
+			}
+		}
+#pragma unroll
+		for (int s = 0; s < WL_VERIFY_SLOTS; s++) {
+			const uint32_t tj = __shfl_sync(mask, tag, sj[s]);
+			const uint32_t d = (x[s].x ^ tj) | (x[s].y ^ tj) | (x[s].z ^ tj) | (x[s].w ^ tj);
+			if (((valid >> s) & 1u) && d)
+				badbits |= 1u << sj[s];
+		}
+	}
+	badbits = __reduce_or_sync(mask, badbits);
+	return bad != 0 || ((badbits >> lane) & 1u);
+}
+#endif
 
 /* Verify every lane's block (p may be NULL) against its tag; true in the
  * owner lane of a block with a word that differs.  Small blocks: each lane
  * reads its own with 16-byte loads unrolled by eight.  Blocks of
- * WL_COOP_BYTES or more: the warp reads each together, up to four vectors
- * per lane, with no synchronisation per block -- mismatches collect in a
- * per-block bit mask reduced once at the end -- so the loads of the whole
- * pass stay in flight instead of one block's at a time. */
-__device__ __forceinline__ bool coop_verify(uint32_t mask, uint32_t lane, const void *p, uint32_t n,
+ * WL_COOP_BYTES or more: the calling lanes read each together, block by
+ * block (each block's loads are consumed before the next block's are
+ * issued, which suits kernels short of registers: the batched form's
+ * measured faster so). */
+__device__ __forceinline__ bool coop_verify_blockwise(uint32_t mask, uint32_t lane, const void *p, uint32_t n,
 		uint32_t tag)
 {
 	const uint32_t *w = (const uint32_t *)p;
@@ -102,17 +201,27 @@ __device__ __forceinline__ bool coop_verify(uint32_t mask, uint32_t lane, const 
 	}
 	uint32_t mb = __ballot_sync(mask, big);
 	uint32_t badbits = 0;
+	const uint32_t width = __popc(mask), rank = __popc(mask & ((1u << lane) - 1u));
 	while (mb) {
 		uint32_t j = __ffs(mb) - 1;
 		mb &= mb - 1;
 		const uint32_t *pj = (const uint32_t *)__shfl_sync(mask, (unsigned long long)w, j);
 		uint32_t nj = __shfl_sync(mask, n, j) >> 2;
 		uint32_t tj = __shfl_sync(mask, tag, j);
-		if (verify_share(lane, pj, nj, tj))
+		if (verify_share(rank, width, pj, nj, tj))
 			badbits |= 1u << j;
 	}
 	badbits = __reduce_or_sync(mask, badbits);
 	return bad != 0 || ((badbits >> lane) & 1u);
+}
+
+__device__ __forceinline__ bool coop_verify(uint32_t mask, uint32_t lane, const void *p, uint32_t n, uint32_t tag)
+{
+#if WL_VERIFY_SLOTS > 0
+	return coop_verify_rows(mask, lane, p, n, tag);
+#else
+	return coop_verify_blockwise(mask, lane, p, n, tag);
+#endif
 }
 
 /* Position of the (k+1)-th set bit of m; requires k < popc(m). */
