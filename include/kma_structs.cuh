@@ -22,6 +22,7 @@
 #define KMA_STRUCTS_CUH
 
 #include "kma_device.cuh"
+#include "kma_queue_algo.h"
 
 #define KMA_STRUCT_SPIN (1u << 20)
 
@@ -41,25 +42,6 @@ __device__ __forceinline__ unsigned long long xchg64_acqrel(unsigned long long *
 	asm volatile("atom.acq_rel.gpu.global.exch.b64 %0, [%1], %2;"
 		     : "=l"(old) : "l"(p), "l"(v) : "memory");
 	return old;
-}
-/* 16-byte compare-and-swap of two adjacent 64-bit words (sm_90+).
- * Returns true when {lo, hi} held {cmp_lo, cmp_hi} and now holds the new
- * pair; p must be 16-byte aligned. */
-__device__ __forceinline__ bool cas128_acqrel(unsigned long long *p, unsigned long long cmp_lo,
-		unsigned long long cmp_hi, unsigned long long val_lo, unsigned long long val_hi)
-{
-	unsigned long long o_lo, o_hi;
-	asm volatile("{\n\t"
-		     ".reg .b128 d, c, v;\n\t"
-		     "mov.b128 c, {%2, %3};\n\t"
-		     "mov.b128 v, {%4, %5};\n\t"
-		     "atom.acq_rel.gpu.global.cas.b128 d, [%6], c, v;\n\t"
-		     "mov.b128 {%0, %1}, d;\n\t"
-		     "}"
-		     : "=l"(o_lo), "=l"(o_hi)
-		     : "l"(cmp_lo), "l"(cmp_hi), "l"(val_lo), "l"(val_hi), "l"(p)
-		     : "memory");
-	return o_lo == cmp_lo && o_hi == cmp_hi;
 }
 /* Exclusive prefix and total of v over the calling lanes (any subset of
  * the warp), in lane order. */
@@ -91,6 +73,25 @@ __device__ __forceinline__ unsigned long long global_thread()
 	return blk * tpb + t;
 }
 
+/* The atomics policy of the queue algorithms (kma_queue_algo.h) on the
+ * GPU: gpu-scope acquire/release PTX. */
+struct gpu_ops {
+	static __device__ __forceinline__ unsigned long long ld(unsigned long long *p) { return ld_acquire64(p); }
+	static __device__ __forceinline__ unsigned long long ld_rlx(unsigned long long *p) { return ld_relaxed64(p); }
+	static __device__ __forceinline__ void st(unsigned long long *p, unsigned long long v) { st_release64(p, v); }
+	static __device__ __forceinline__ void st_rlx(unsigned long long *p, unsigned long long v) { st_relaxed64(p, v); }
+	static __device__ __forceinline__ unsigned long long xchg(unsigned long long *p, unsigned long long v)
+	{
+		return xchg64_acqrel(p, v);
+	}
+	static __device__ __forceinline__ unsigned long long cas(unsigned long long *p, unsigned long long c,
+			unsigned long long v)
+	{
+		return cas64_acqrel(p, c, v);
+	}
+	static __device__ __forceinline__ void pause(uint32_t it) { backoff(it); }
+};
+
 } /* namespace kma_detail */
 
 /* ================================================================== */
@@ -105,16 +106,19 @@ __device__ __forceinline__ unsigned long long global_thread()
  * as the reference does (clQueue.cl:97), so a removed item keeps POISON in
  * its link until it is enqueued again.
  *
- * Different from the reference, which under concurrency can leave `tail`
- * on an item that was already dequeued (a dequeue of the last item racing
- * an enqueue behind it, clQueue.cl:60-66 vs :106-108), after which every
- * enqueue spins:
- *   - head and tail carry 16-bit tags above a 48-bit pointer, so a stale
- *     CAS on either fails (ABA);
- *   - the empty <-> one-item transitions change head and tail together
- *     with one 16-byte CAS;
- *   - a dequeue that moves head past the item tail points at moves tail
- *     on (helping), so tail never points at a removed item.
+ * The algorithm is kma_queue_algo.h's (the text its host harness checks):
+ *   - enqueue exchanges the tail (always succeeds, one atomic), then links
+ *     the previous tail item to the new one; the reference CASes the tail
+ *     item's link in a retry loop and then the tail (clQueue.cl:40-75), so
+ *     on one hot queue every enqueue but one per round trip retries;
+ *   - a warp's items for one queue go in as one chain, one exchange
+ *     (kma_clqueue_enqueue_warp), and a warp's dequeues of one queue take
+ *     consecutive items under one hold of the head (kma_clqueue_dequeue_warp);
+ *   - head carries a 16-bit tag above the 48-bit pointer, so a stale CAS
+ *     fails (ABA); the dequeue that empties the queue clears the tail with
+ *     a CAS, so an append racing it is never lost -- the reference can
+ *     leave `tail` on an already dequeued item there (clQueue.cl:60-66 vs
+ *     :106-108), after which every enqueue spins.
  * Items must stay queue items (type-stable memory) while any thread may
  * still hold a pointer to them, as in the reference (clQueue.cl:92-96).
  * Device pointers must be below 2^48 (the tag bits); enqueue refuses
@@ -122,7 +126,7 @@ __device__ __forceinline__ unsigned long long global_thread()
  */
 struct __align__(16) kma_clqueue {
 	unsigned long long head; /* {tag:16 | item ptr:48} */
-	unsigned long long tail;
+	unsigned long long tail; /* the last item's pointer, 0 when empty */
 };
 struct kma_clqueue_item {
 	unsigned long long next; /* item ptr, 0 = end, 1 = POISON */
@@ -168,57 +172,21 @@ struct clq_link_aligned {
 	static __device__ __forceinline__ bool ok(unsigned long long) { return true; }
 };
 
-#ifndef KMA_CONTEND_MAX_NS
-#define KMA_CONTEND_MAX_NS 4096u
-#endif
-/* After a CAS lost to another thread on a contended word: a randomised
- * exponential wait (__nanosleep(t) sleeps somewhere in [0, 2t]), 64 ns
- * doubling per consecutive loss up to KMA_CONTEND_MAX_NS.  Retrying at
- * once floods the word's L2 slice with requests that queue ahead of the
- * winner's next step; spread out, the retries let one thread through per
- * round trip. */
-__device__ __forceinline__ void contend(uint32_t &losses)
+template <class L>
+__device__ __forceinline__ bool clq_item_ok(unsigned long long it_p)
 {
-	uint32_t t = 64u << (losses < 10 ? losses : 10);
-	__nanosleep(t < KMA_CONTEND_MAX_NS ? t : KMA_CONTEND_MAX_NS);
-	losses++;
+	return it_p != 0 && it_p != KMA_Q_POISON && !(it_p & ~KMA_PTR_MASK) && L::ok(it_p);
 }
 
 template <class L>
 __device__ inline int clq_enqueue(kma_clqueue *q, unsigned long long it_p, uint32_t *err, uint32_t spin_limit)
 {
-	if (it_p == 0 || it_p == KMA_Q_POISON || (it_p & ~KMA_PTR_MASK) || !L::ok(it_p))
+	if (!clq_item_ok<L>(it_p))
 		return 0;
-	st_release64(L::at(it_p), 0ull);
-	uint32_t losses = 0;
-	for (uint32_t it = 0; it < spin_limit; it++) {
-		unsigned long long t = ld_acquire64(&q->tail);
-		if (qp_ptr(t) == 0) {
-			unsigned long long h = ld_acquire64(&q->head);
-			if (qp_ptr(h) == 0 &&
-			    cas128_acqrel(&q->head, h, t, qp_next(h, it_p), qp_next(t, it_p)))
-				return 1;
-			backoff(it);
-			continue;
-		}
-		unsigned long long *tl = L::at(qp_ptr(t));
-		unsigned long long n = ld_acquire64(tl);
-		if (t != ld_acquire64(&q->tail))
-			continue;
-		if (n == 0) {
-			if (cas64_acqrel(tl, 0ull, it_p) == 0ull) {
-				cas64_acqrel(&q->tail, t, qp_next(t, it_p));
-				return 1;
-			}
-			contend(losses);
-		} else if (n == KMA_Q_POISON) {
-			/* the tail item is being dequeued: it either goes (the
-			 * queue empties) or its link comes back */
-			backoff(it);
-		} else {
-			cas64_acqrel(&q->tail, t, qp_next(t, n)); /* help the lagging tail */
-		}
-	}
+	/* the link is published by the exchange (acq_rel) that appends it */
+	st_relaxed64(L::at(it_p), 0ull);
+	if (kma_q::clq_append<gpu_ops, L>(&q->head, &q->tail, it_p, it_p, spin_limit))
+		return 1;
 	flag_err(err, KMA_ERR_TIMEOUT);
 	return 0;
 }
@@ -226,37 +194,12 @@ __device__ inline int clq_enqueue(kma_clqueue *q, unsigned long long it_p, uint3
 template <class L>
 __device__ inline unsigned long long clq_dequeue(kma_clqueue *q, uint32_t *err, uint32_t spin_limit)
 {
-	for (uint32_t it = 0; it < spin_limit; it++) {
-		unsigned long long h = ld_acquire64(&q->head);
-		unsigned long long hp = qp_ptr(h);
-		if (hp == 0)
-			return 0;
-		unsigned long long *hl = L::at(hp);
-		unsigned long long nx = xchg64_acqrel(hl, KMA_Q_POISON);
-		if (nx == KMA_Q_POISON) {
-			/* another dequeuer holds it, or it was removed already */
-			backoff(it);
-			continue;
-		}
-		if (nx != 0) {
-			if (cas64_acqrel(&q->head, h, qp_next(h, nx)) == h) {
-				unsigned long long t = ld_acquire64(&q->tail);
-				if (qp_ptr(t) == hp)
-					cas64_acqrel(&q->tail, t, qp_next(t, nx));
-				return hp;
-			}
-		} else {
-			/* the last item: head and tail go to NULL together, which
-			 * fails if tail has not reached it yet */
-			unsigned long long t = ld_acquire64(&q->tail);
-			if (qp_ptr(t) == hp && cas128_acqrel(&q->head, h, t, qp_next(h, 0), qp_next(t, 0)))
-				return hp;
-		}
-		/* stale head: put the link back (clQueue.cl:113) */
-		cas64_acqrel(hl, KMA_Q_POISON, nx);
-		backoff(it);
-	}
-	flag_err(err, KMA_ERR_TIMEOUT);
+	unsigned long long out = 0;
+	bool timed_out = false;
+	if (kma_q::clq_dequeue_n<gpu_ops, L>(&q->head, &q->tail, &out, 1, spin_limit, &timed_out))
+		return out;
+	if (timed_out)
+		flag_err(err, KMA_ERR_TIMEOUT);
 	return 0;
 }
 
@@ -265,6 +208,25 @@ __device__ __forceinline__ unsigned long long clq_next(unsigned long long p)
 {
 	unsigned long long n = *(const volatile unsigned long long *)L::at(p);
 	return n == KMA_Q_POISON ? 0ull : n;
+}
+
+/* Lanes grouped by key: this lane's group (lanes with the same key among
+ * the `active` lanes), its rank and size, the group's first and last
+ * lanes, and the next lane of the group above this one (or this lane). */
+struct lane_group {
+	uint32_t peers, rank, size, first, last, next;
+};
+__device__ __forceinline__ lane_group group_by(uint32_t active, uint32_t lane, unsigned long long key)
+{
+	lane_group gp;
+	gp.peers = __match_any_sync(active, key);
+	gp.rank = __popc(gp.peers & ((1u << lane) - 1u));
+	gp.size = __popc(gp.peers);
+	gp.first = __ffs(gp.peers) - 1;
+	gp.last = 31 - __clz(gp.peers);
+	const uint32_t above = lane == 31 ? 0u : gp.peers & ~((2u << lane) - 1u);
+	gp.next = above ? __ffs(above) - 1 : lane;
+	return gp;
 }
 } /* namespace kma_detail */
 
@@ -283,6 +245,82 @@ __device__ __forceinline__ kma_clqueue_item *kma_clqueue_dequeue(kma_clqueue *q,
 {
 	return reinterpret_cast<kma_clqueue_item *>(
 		kma_detail::clq_dequeue<kma_detail::clq_link_head>(q, err, spin_limit));
+}
+
+/* Warp form of enqueue: every calling lane appends its own item (NULL: no
+ * item) to its own queue (lanes may name different queues).  The items of
+ * one queue are linked in lane order and appended as one chain with one
+ * exchange of its tail, so they come out in lane order, together.  Returns
+ * what kma_clqueue_enqueue would for the lane's item (1, or 0 for a
+ * refused item or an expired wait).  No counterpart in the reference. */
+__device__ inline int kma_clqueue_enqueue_warp(kma_clqueue *q, kma_clqueue_item *item, uint32_t *err = nullptr,
+		uint32_t spin_limit = KMA_STRUCT_SPIN)
+{
+	using namespace kma_detail;
+	const uint32_t active = __activemask();
+	const uint32_t lane = lane_id();
+	const unsigned long long ip = (unsigned long long)item;
+	const bool ok = q && clq_item_ok<clq_link_head>(ip);
+	const lane_group gp = group_by(active, lane, ok ? (unsigned long long)q : ~0ull);
+	const unsigned long long nip = __shfl_sync(active, ip, gp.next);
+	const unsigned long long lip = __shfl_sync(active, ip, gp.last);
+	if (ok) {
+		st_relaxed64(clq_link_head::at(ip), gp.next != lane ? nip : 0ull);
+		/* every lane's link is visible before the first lane's exchange
+		 * publishes the chain */
+		__threadfence();
+	}
+	__syncwarp(active);
+	int r = 0;
+	if (ok && lane == gp.first) {
+		r = kma_q::clq_append<gpu_ops, clq_link_head>(&q->head, &q->tail, ip, lip, spin_limit);
+		if (!r)
+			flag_err(err, KMA_ERR_TIMEOUT);
+	}
+	r = __shfl_sync(active, r, gp.first);
+	return ok ? r : 0;
+}
+
+/* Warp form of dequeue: every calling lane takes one item from its own
+ * queue (NULL q: none).  The lanes of one queue take consecutive items
+ * under one hold of its head, in lane order; lanes left over when the
+ * queue runs empty get NULL.  No counterpart in the reference. */
+__device__ inline kma_clqueue_item *kma_clqueue_dequeue_warp(kma_clqueue *q, uint32_t *err = nullptr,
+		uint32_t spin_limit = KMA_STRUCT_SPIN)
+{
+	using namespace kma_detail;
+	const uint32_t active = __activemask();
+	const uint32_t lane = lane_id();
+	const lane_group gp = group_by(active, lane, q ? (unsigned long long)q : ~0ull);
+	unsigned long long got = 0;
+	uint32_t served = 0;
+	bool more = q != nullptr;
+	/* one batch per turn; a group's turns end when it is served or the
+	 * queue is empty */
+	for (uint32_t turn = 0; __any_sync(active, more) && turn < 32; turn++) {
+		unsigned long long out[32];
+		uint32_t r = 0;
+		if (more && lane == gp.first) {
+			bool timed_out = false;
+			r = kma_q::clq_dequeue_n<gpu_ops, clq_link_head>(&q->head, &q->tail, out, gp.size - served,
+									 spin_limit, &timed_out);
+			if (timed_out)
+				flag_err(err, KMA_ERR_TIMEOUT);
+		}
+		r = __shfl_sync(active, r, gp.first);
+		const uint32_t rmax = __reduce_max_sync(active, more ? r : 0u);
+		for (uint32_t j = 0; j < rmax; j++) {
+			const unsigned long long v = __shfl_sync(active, lane == gp.first && j < r ? out[j] : 0ull, gp.first);
+			if (more && j < r && gp.rank == served + j)
+				got = v;
+		}
+		if (more) {
+			served += r;
+			if (r == 0 || served >= gp.size)
+				more = false;
+		}
+	}
+	return reinterpret_cast<kma_clqueue_item *>(got);
 }
 
 /* The first item (NULL when empty), for walks from the head. */
@@ -306,12 +344,18 @@ __device__ __forceinline__ kma_clqueue_item *kma_clqueue_next(const kma_clqueue_
  * An item's first 8 bytes are its link, a {tag:32 | index:32} word (the
  * reference packs {tag:10 | index:16 | poison:1} into 32 bits,
  * clIndexedQueue.cl:90-92, so it holds at most 65 535 items and wraps its
- * tag every 1024 updates).  Head and tail are tagged the same way, each on
- * its own 128-byte line, and every update increments the tag, so no CAS
- * succeeds on a recycled value.  The algorithm is the Michael-Scott queue
- * with a dummy item, as the reference's: init makes `first` the dummy,
- * dequeue returns the OLD dummy (so `first` comes out first and the last
- * item enqueued always stays behind), NULL when only the dummy is left.
+ * tag every 1024 updates).  Head is tagged the same way, on its own
+ * 128-byte line, and every update increments the tag, so no CAS succeeds
+ * on a recycled value; the tail, on its own line, holds the last item's
+ * index.  The queue is the Michael-Scott queue with a dummy item, as the
+ * reference's: init makes `first` the dummy, dequeue returns the OLD dummy
+ * (so `first` comes out first and the last item enqueued always stays
+ * behind), NULL when only the dummy is left.  The algorithm is
+ * kma_queue_algo.h's: enqueue exchanges the tail and links the previous
+ * tail item (no retry loop, one atomic on the shared tail, where the
+ * reference CASes the link and then the tail, clIndexedQueue.cl:132-196);
+ * the warp forms append a warp's items as one chain and take a warp's
+ * dequeues with one CAS of the head.
  *
  * Shards (B200 addition, default 1): `nshards` independent queues over
  * the same item array, chosen by global thread id % nshards, so a
@@ -373,67 +417,48 @@ __device__ __forceinline__ void *kma_iqueue_item(const kma_iqueue *q, uint32_t i
 	return q->base + ((size_t)(idx - 1) << q->stride_l2);
 }
 
+namespace kma_detail {
+/* the item links of q, as the queue algorithms address them */
+struct iq_links {
+	const kma_iqueue *q;
+	__device__ __forceinline__ unsigned long long *link(uint32_t idx) const { return iq_link(q, idx); }
+};
+} /* namespace kma_detail */
+
 /* idxd_enqueue (clIndexedQueue.cl:132-196) on the caller's shard: 1 on
- * success, 0 for an item outside the array or on spin-limit expiry. */
+ * success, 0 for an item outside the array.  Never waits. */
 __device__ inline int kma_iqueue_enqueue_shard(kma_iqueue *q, void *item, uint32_t shard)
 {
 	using namespace kma_detail;
 	uint32_t idx = iq_idx(q, item);
 	if (idx == 0)
 		return 0;
-	unsigned long long *link = iq_link(q, idx);
-	unsigned long long old = *((volatile unsigned long long *)link);
-	st_release64(link, tw_make(tw_tag(old) + 1, 0));
-	unsigned long long *tailw = &q->ends[2 * shard + 1].v;
-	uint32_t lim = q->spin_limit;
-	for (uint32_t it = 0; it < lim; it++) {
-		unsigned long long t = ld_acquire64(tailw);
-		unsigned long long *tl = iq_link(q, tw_idx(t));
-		unsigned long long n = ld_acquire64(tl);
-		if (t != ld_acquire64(tailw))
-			continue;
-		if (tw_idx(n) == 0) {
-			if (cas64_acqrel(tl, n, tw_make(tw_tag(n) + 1, idx)) == n) {
-				cas64_acqrel(tailw, t, tw_make(tw_tag(t) + 1, idx));
-				return 1;
-			}
-		} else {
-			cas64_acqrel(tailw, t, tw_make(tw_tag(t) + 1, tw_idx(n)));
-		}
-		backoff(it);
-	}
-	atomicOr(&q->err, KMA_ERR_TIMEOUT);
-	return 0;
+	const iq_links L{q};
+	kma_q::iq_set_link<gpu_ops>(L, idx, 0u);
+	/* the link is published by the exchange (acq_rel) that appends it */
+	kma_q::iq_append<gpu_ops>(L, &q->ends[2 * shard + 1].v, idx, idx);
+	return 1;
 }
 
 /* idxd_dequeue (clIndexedQueue.cl:203-247) on one shard: the old dummy
  * (an item pointer), NULL when only the dummy is left or on spin-limit
- * expiry. */
+ * expiry.  An internal dummy leaving the shard is skipped. */
 __device__ inline void *kma_iqueue_dequeue_shard(kma_iqueue *q, uint32_t shard)
 {
 	using namespace kma_detail;
-	unsigned long long *headw = &q->ends[2 * shard].v;
-	unsigned long long *tailw = &q->ends[2 * shard + 1].v;
-	uint32_t lim = q->spin_limit;
-	for (uint32_t it = 0; it < lim; it++) {
-		unsigned long long hd = ld_acquire64(headw);
-		unsigned long long t = ld_acquire64(tailw);
-		unsigned long long n = ld_acquire64(iq_link(q, tw_idx(hd)));
-		if (hd != ld_acquire64(headw))
-			continue;
-		if (tw_idx(hd) == tw_idx(t)) {
-			if (tw_idx(n) == 0)
-				return nullptr;
-			cas64_acqrel(tailw, t, tw_make(tw_tag(t) + 1, tw_idx(n)));
-		} else if (cas64_acqrel(headw, hd, tw_make(tw_tag(hd) + 1, tw_idx(n))) == hd) {
-			uint32_t idx = tw_idx(hd);
-			if (idx > q->capacity)
-				continue; /* an internal dummy left the shard: take the next item */
-			return kma_iqueue_item(q, idx);
+	const iq_links L{q};
+	for (uint32_t k = 0; k < 2; k++) {
+		uint32_t idx = 0;
+		bool timed_out = false;
+		if (!kma_q::iq_dequeue_n<gpu_ops>(L, &q->ends[2 * shard].v, &idx, 1, q->spin_limit, &timed_out)) {
+			if (timed_out)
+				atomicOr(&q->err, KMA_ERR_TIMEOUT);
+			return nullptr;
 		}
-		backoff(it);
+		if (idx <= q->capacity)
+			return kma_iqueue_item(q, idx);
+		/* shard k > 0's initial internal dummy: at most once per shard */
 	}
-	atomicOr(&q->err, KMA_ERR_TIMEOUT);
 	return nullptr;
 }
 
@@ -444,6 +469,93 @@ __device__ __forceinline__ int kma_iqueue_enqueue(kma_iqueue *q, void *item)
 __device__ __forceinline__ void *kma_iqueue_dequeue(kma_iqueue *q)
 {
 	return kma_iqueue_dequeue_shard(q, kma_detail::iq_shard(q));
+}
+
+/* Warp form of enqueue on each lane's shard (NULL item: none): the items
+ * of one shard are linked in lane order and appended as one chain with
+ * one exchange of its tail.  1 per appended item, 0 for an item outside
+ * the array.  No counterpart in the reference. */
+__device__ inline int kma_iqueue_enqueue_warp_shard(kma_iqueue *q, void *item, uint32_t shard)
+{
+	using namespace kma_detail;
+	const uint32_t active = __activemask();
+	const uint32_t lane = lane_id();
+	const uint32_t idx = item ? iq_idx(q, item) : 0u;
+	const bool ok = idx != 0;
+	const lane_group gp = group_by(active, lane, ok ? (unsigned long long)shard : ~0ull);
+	const uint32_t nidx = __shfl_sync(active, idx, gp.next);
+	const uint32_t lidx = __shfl_sync(active, idx, gp.last);
+	const iq_links L{q};
+	if (ok) {
+		kma_q::iq_set_link<gpu_ops>(L, idx, gp.next != lane ? nidx : 0u);
+		/* every lane's link is visible before the first lane's exchange
+		 * publishes the chain */
+		__threadfence();
+	}
+	__syncwarp(active);
+	if (ok && lane == gp.first)
+		kma_q::iq_append<gpu_ops>(L, &q->ends[2 * shard + 1].v, idx, lidx);
+	return ok ? 1 : 0;
+}
+
+/* Warp form of dequeue on each lane's shard (want 0: none): the lanes of
+ * one shard take consecutive old dummies with one CAS of its head, in lane
+ * order; lanes left over when only the dummy is left get NULL.  No
+ * counterpart in the reference. */
+__device__ inline void *kma_iqueue_dequeue_warp_shard(kma_iqueue *q, uint32_t shard, bool want = true)
+{
+	using namespace kma_detail;
+	const uint32_t active = __activemask();
+	const uint32_t lane = lane_id();
+	const lane_group gp = group_by(active, lane, want ? (unsigned long long)shard : ~0ull);
+	const iq_links L{q};
+	uint32_t got = 0, served = 0;
+	bool more = want;
+	for (uint32_t turn = 0; __any_sync(active, more) && turn < 33; turn++) {
+		uint32_t out[32];
+		uint32_t r = 0;
+		if (more && lane == gp.first) {
+			bool timed_out = false;
+			r = kma_q::iq_dequeue_n<gpu_ops>(L, &q->ends[2 * shard].v, out, gp.size - served, q->spin_limit,
+							 &timed_out);
+			if (timed_out)
+				atomicOr(&q->err, KMA_ERR_TIMEOUT);
+			/* internal dummies leave silently */
+			uint32_t k = 0;
+			for (uint32_t j = 0; j < r; j++)
+				if (out[j] <= q->capacity)
+					out[k++] = out[j];
+			if (r && !k)
+				r = ~0u; /* only an internal dummy left: take again */
+			else
+				r = k;
+		}
+		r = __shfl_sync(active, r, gp.first);
+		const bool again = r == ~0u;
+		if (again)
+			r = 0;
+		const uint32_t rmax = __reduce_max_sync(active, more ? r : 0u);
+		for (uint32_t j = 0; j < rmax; j++) {
+			const uint32_t v = __shfl_sync(active, lane == gp.first && j < r ? out[j] : 0u, gp.first);
+			if (more && j < r && gp.rank == served + j)
+				got = v;
+		}
+		if (more && !again) {
+			served += r;
+			if (r == 0 || served >= gp.size)
+				more = false;
+		}
+	}
+	return got ? kma_iqueue_item(q, got) : nullptr;
+}
+
+__device__ __forceinline__ int kma_iqueue_enqueue_warp(kma_iqueue *q, void *item)
+{
+	return kma_iqueue_enqueue_warp_shard(q, item, kma_detail::iq_shard(q));
+}
+__device__ __forceinline__ void *kma_iqueue_dequeue_warp(kma_iqueue *q)
+{
+	return kma_iqueue_dequeue_warp_shard(q, kma_detail::iq_shard(q));
 }
 
 /* ================================================================== */

@@ -137,6 +137,11 @@ int kma_clarraylist_group_host(kma_heap_t kma, kma_pma_t pma, uint32_t obj_size,
 /* ---- concurrent microbenchmarks -------------------------------------- */
 #define KMA_C3_CLQUEUE 0
 #define KMA_C3_IQUEUE 1
+/* or'ed into the kind: every enqueue and dequeue through the warp forms
+ * (kma_clqueue_enqueue_warp / _dequeue_warp, kma_iqueue_enqueue_warp_shard
+ * / _dequeue_warp_shard): a warp's items for one queue go in as one chain
+ * and its dequeues take consecutive items together */
+#define KMA_C3_WARP 0x100
 
 typedef struct kma_c3_queue_stats {
 	uint64_t enqueued;       /* successful enqueues */

@@ -800,6 +800,7 @@ __device__ __forceinline__ void warp_flush(unsigned long long *dst, unsigned lon
 
 /* acc: [0..2] in (count, xor, sum), [3..5] out, [6] empty, [7] remaining,
  * [8] walk failures */
+template <bool WARP>
 __global__ void k_c3_clq_enq(unsigned char *qs, uint32_t shards, unsigned char *items, uint32_t per_thread,
 		uint32_t n, uint64_t seed, unsigned long long *acc, uint32_t *err)
 {
@@ -808,12 +809,16 @@ __global__ void k_c3_clq_enq(unsigned char *qs, uint32_t shards, unsigned char *
 	kma_clqueue *q = (kma_clqueue *)(qs + (size_t)(t % shards) * 128);
 	for (uint32_t k = 0; k < per_thread; k++) {
 		uint32_t i = t * per_thread + k;
-		if (i >= n)
+		/* the warp form keeps every lane in the loop (NULL: no item) */
+		if (!WARP && i >= n)
 			break;
-		unsigned char *it = items + (size_t)i * QITEM;
-		uint32_t pay = perm_u32(i, n, seed);
-		*(uint32_t *)(it + 8) = pay;
-		if (kma_clqueue_enqueue(q, (kma_clqueue_item *)it, err)) {
+		unsigned char *it = i < n ? items + (size_t)i * QITEM : nullptr;
+		uint32_t pay = i < n ? perm_u32(i, n, seed) : 0u;
+		if (it)
+			*(uint32_t *)(it + 8) = pay;
+		int ok = WARP ? kma_clqueue_enqueue_warp(q, (kma_clqueue_item *)it, err)
+			      : kma_clqueue_enqueue(q, (kma_clqueue_item *)it, err);
+		if (ok) {
 			c++;
 			x ^= pay;
 			s += pay;
@@ -822,15 +827,18 @@ __global__ void k_c3_clq_enq(unsigned char *qs, uint32_t shards, unsigned char *
 	warp_flush(acc, c, x, s);
 }
 
+template <bool WARP>
 __global__ void k_c3_clq_deq(unsigned char *qs, uint32_t shards, uint32_t per_thread, uint32_t threads,
 		unsigned long long *acc, uint32_t *err)
 {
 	uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
 	unsigned long long c = 0, x = 0, s = 0, e = 0;
-	if (t < threads) {
-		kma_clqueue *q = (kma_clqueue *)(qs + (size_t)(t % shards) * 128);
+	if (WARP || t < threads) {
+		kma_clqueue *q = t < threads ? (kma_clqueue *)(qs + (size_t)(t % shards) * 128) : nullptr;
 		for (uint32_t k = 0; k < per_thread; k++) {
-			kma_clqueue_item *it = kma_clqueue_dequeue(q, err);
+			kma_clqueue_item *it = WARP ? kma_clqueue_dequeue_warp(q, err) : kma_clqueue_dequeue(q, err);
+			if (!q)
+				continue;
 			if (!it) {
 				e++;
 				continue;
@@ -879,6 +887,7 @@ __global__ void k_c3_clq_walk(unsigned char *qs, uint32_t shards, uint64_t n, un
 }
 
 /* indexed queue: item 0 is shard 0's initial dummy (payload excluded) */
+template <bool WARP>
 __global__ void k_c3_iq_enq(kma_iqueue *q, uint32_t per_thread, uint32_t n, uint64_t seed, unsigned long long *acc)
 {
 	uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -886,12 +895,13 @@ __global__ void k_c3_iq_enq(kma_iqueue *q, uint32_t per_thread, uint32_t n, uint
 	uint32_t shard = t % q->nshards;
 	for (uint32_t k = 0; k < per_thread; k++) {
 		uint32_t i = t * per_thread + k;
-		if (i >= n)
+		if (!WARP && i >= n)
 			break;
-		unsigned char *it = q->base + ((size_t)(i + 1) << q->stride_l2);
-		uint32_t pay = perm_u32(i, n, seed);
-		*(uint32_t *)(it + 8) = pay;
-		if (kma_iqueue_enqueue_shard(q, it, shard)) {
+		unsigned char *it = i < n ? q->base + ((size_t)(i + 1) << q->stride_l2) : nullptr;
+		uint32_t pay = i < n ? perm_u32(i, n, seed) : 0u;
+		if (it)
+			*(uint32_t *)(it + 8) = pay;
+		if (WARP ? kma_iqueue_enqueue_warp_shard(q, it, shard) : kma_iqueue_enqueue_shard(q, it, shard)) {
 			c++;
 			x ^= pay;
 			s += pay;
@@ -900,14 +910,18 @@ __global__ void k_c3_iq_enq(kma_iqueue *q, uint32_t per_thread, uint32_t n, uint
 	warp_flush(acc, c, x, s);
 }
 
+template <bool WARP>
 __global__ void k_c3_iq_deq(kma_iqueue *q, uint32_t per_thread, uint32_t threads, unsigned long long *acc)
 {
 	uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
 	unsigned long long c = 0, x = 0, s = 0, e = 0, d0 = 0;
-	if (t < threads) {
+	if (WARP || t < threads) {
 		uint32_t shard = t % q->nshards;
 		for (uint32_t k = 0; k < per_thread; k++) {
-			unsigned char *it = (unsigned char *)kma_iqueue_dequeue_shard(q, shard);
+			unsigned char *it = WARP ? (unsigned char *)kma_iqueue_dequeue_warp_shard(q, shard, t < threads)
+						 : (unsigned char *)kma_iqueue_dequeue_shard(q, shard);
+			if (t >= threads)
+				continue;
 			if (!it) {
 				e++;
 				continue;
@@ -970,6 +984,8 @@ __global__ void k_c3_iq_walk(kma_iqueue *q, uint64_t n, unsigned long long *acc)
 extern "C" int kma_c3_queue_run(int kind, uint32_t threads, uint32_t per_thread, uint32_t shards, uint64_t seed,
 		int device, kma_c3_queue_stats *st)
 {
+	const bool warp = kind & KMA_C3_WARP;
+	kind &= ~KMA_C3_WARP;
 	if (!st || threads == 0 || per_thread == 0 || shards == 0 || shards > KMA_IQ_MAX_SHARDS ||
 	    (kind != KMA_C3_CLQUEUE && kind != KMA_C3_IQUEUE))
 		return KMA_EINVAL;
@@ -1004,9 +1020,15 @@ extern "C" int kma_c3_queue_run(int kind, uint32_t threads, uint32_t per_thread,
 		if (rc == KMA_OK) {
 			cudaMemset(qs, 0, (size_t)shards * 128);
 			cudaEventRecord(e0);
-			k_c3_clq_enq<<<blocks, 256>>>(qs, shards, items, per_thread, n, seed, acc, err);
+			if (warp)
+				k_c3_clq_enq<true><<<blocks, 256>>>(qs, shards, items, per_thread, n, seed, acc, err);
+			else
+				k_c3_clq_enq<false><<<blocks, 256>>>(qs, shards, items, per_thread, n, seed, acc, err);
 			cudaEventRecord(e1);
-			k_c3_clq_deq<<<blocks, 256>>>(qs, shards, per_thread, threads, acc, err);
+			if (warp)
+				k_c3_clq_deq<true><<<blocks, 256>>>(qs, shards, per_thread, threads, acc, err);
+			else
+				k_c3_clq_deq<false><<<blocks, 256>>>(qs, shards, per_thread, threads, acc, err);
 			cudaEventRecord(e2);
 			k_c3_clq_walk<<<(shards + 127) / 128, 128>>>(qs, shards, n, acc);
 		}
@@ -1014,9 +1036,15 @@ extern "C" int kma_c3_queue_run(int kind, uint32_t threads, uint32_t per_thread,
 		rc = kma_iqueue_create(items, 4, n + 1, items, shards, -1, NULL, &iq);
 		if (rc == KMA_OK) {
 			cudaEventRecord(e0);
-			k_c3_iq_enq<<<blocks, 256>>>(iq->dq, per_thread, n, seed, acc);
+			if (warp)
+				k_c3_iq_enq<true><<<blocks, 256>>>(iq->dq, per_thread, n, seed, acc);
+			else
+				k_c3_iq_enq<false><<<blocks, 256>>>(iq->dq, per_thread, n, seed, acc);
 			cudaEventRecord(e1);
-			k_c3_iq_deq<<<blocks, 256>>>(iq->dq, per_thread, threads, acc);
+			if (warp)
+				k_c3_iq_deq<true><<<blocks, 256>>>(iq->dq, per_thread, threads, acc);
+			else
+				k_c3_iq_deq<false><<<blocks, 256>>>(iq->dq, per_thread, threads, acc);
 			cudaEventRecord(e2);
 			k_c3_iq_walk<<<(shards + 127) / 128, 128>>>(iq->dq, n, acc);
 		}

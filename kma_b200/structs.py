@@ -20,6 +20,7 @@ from .heap import Heap, _stream_ptr
 
 C3_CLQUEUE = 0
 C3_IQUEUE = 1
+C3_WARP = 0x100  # or into the kind: warp-combined enqueues and dequeues
 
 
 class _Handle:
