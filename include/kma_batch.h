@@ -41,6 +41,9 @@ typedef struct kma_batch_stats {
 	uint64_t cache_hits;  /* mallocs served by the warp cache */
 	uint64_t cache_puts;  /* frees kept by the warp cache */
 	uint64_t retired;     /* blocks freed early because a thread's table was full */
+	uint64_t refused;     /* NULL mallocs whose size exceeds the heap's largest
+			       * request (superblock - 16); `nulls` counts them too,
+			       * the rest of `nulls` found the heap exhausted */
 } kma_batch_stats;
 
 #define KMA_BATCH_MAX_CACHE 8
@@ -64,7 +67,9 @@ int kma_batch_launch(kma_batch_t b, void *stream);
 int kma_batch_stats_get(kma_batch_t b, void *stream, kma_batch_stats *out);
 
 typedef struct kma_batch_tune_entry {
-	uint32_t sb_size_log2, block_dim, cache_depth, pad;
+	uint32_t sb_size_log2, block_dim, cache_depth;
+	uint32_t serves_all;   /* 1 when the superblock size serves every size the
+				* jobs draw (up to 4096 bytes); only such entries win */
 	float ms;              /* mean device time of one captured run */
 	float mops;            /* (mallocs + frees) / time, M ops/s */
 	kma_batch_stats stats; /* of the last timed run */
@@ -76,8 +81,10 @@ typedef struct kma_batch_tune_entry {
  * the heap default), capture the run as a graph, launch it `warmup` times untimed and
  * `reps` times timed (CUDA events), and record the entry; *best is the
  * index of the configuration with the most successful calls per second
- * (mallocs that returned a block, plus frees) among those whose runs kept
- * every tag intact and set no heap error flag.
+ * (mallocs that returned a block, plus frees) among those whose superblock
+ * size serves every size the jobs draw (4 KiB superblocks serve at most
+ * 4080 bytes, so they cannot) and whose runs kept every tag intact and set
+ * no heap error flag; 0xffffffff when none qualifies.
  * entries must hold n_sb * n_bd * n_depth entries. */
 int kma_batch_autotune(const kma_batch_job *jobs, uint32_t njobs, uint32_t rounds, uint64_t heap_bytes,
 		       uint32_t shards,

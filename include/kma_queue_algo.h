@@ -115,6 +115,12 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 		if (hp == 0)
 			return 0;
 		u64 *hl = L::at(hp);
+		/* look before taking: while another dequeuer holds the head item,
+		 * waiters only read its link */
+		if (O::ld_rlx(hl) == POISON) {
+			O::pause(it++);
+			continue;
+		}
 		const u64 nx = O::xchg(hl, POISON);
 		if (nx == POISON) {
 			/* another dequeuer holds it, or it left the queue already */

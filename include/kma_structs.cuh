@@ -89,7 +89,15 @@ struct gpu_ops {
 	{
 		return cas64_acqrel(p, c, v);
 	}
-	static __device__ __forceinline__ void pause(uint32_t it) { backoff(it); }
+	/* after `it` fruitless tries: a randomised wait (__nanosleep(t) sleeps
+	 * somewhere in [0, 2t]) of 64 ns doubling per try, at most 4 us, so
+	 * that the waiters on one hot word do not flood its L2 slice with
+	 * requests queued ahead of the holder's */
+	static __device__ __forceinline__ void pause(uint32_t it)
+	{
+		const uint32_t t = 64u << (it < 6 ? it : 6);
+		__nanosleep(t);
+	}
 };
 
 } /* namespace kma_detail */

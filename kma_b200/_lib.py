@@ -81,12 +81,12 @@ class KmaBatchJob(Structure):
 class KmaBatchStats(Structure):
     _fields_ = [("mallocs", c_uint64), ("frees", c_uint64), ("nulls", c_uint64), ("bad_tags", c_uint64),
                 ("fill_bytes", c_uint64), ("verify_bytes", c_uint64), ("cache_hits", c_uint64),
-                ("cache_puts", c_uint64), ("retired", c_uint64)]
+                ("cache_puts", c_uint64), ("retired", c_uint64), ("refused", c_uint64)]
 
 
 class KmaBatchTuneEntry(Structure):
     _fields_ = [("sb_size_log2", c_uint32), ("block_dim", c_uint32), ("cache_depth", c_uint32),
-                ("pad", c_uint32), ("ms", c_float), ("mops", c_float), ("stats", KmaBatchStats)]
+                ("serves_all", c_uint32), ("ms", c_float), ("mops", c_float), ("stats", KmaBatchStats)]
 
 
 class KmaServeCfg(Structure):

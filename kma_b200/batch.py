@@ -95,5 +95,7 @@ def autotune(threads, seeds, rounds: int, heap_bytes: int, sb_log2s=(12, 14, 16)
     out = []
     for e in ent:
         out.append({"sb_size": 1 << e.sb_size_log2, "block_dim": e.block_dim, "cache_depth": e.cache_depth,
-                    "ms": round(e.ms, 3), "mops": round(e.mops, 1), **_stats(e.stats)})
-    return out, int(best.value)
+                    "serves_all": bool(e.serves_all), "ms": round(e.ms, 3), "mops": round(e.mops, 1),
+                    **_stats(e.stats)})
+    b = int(best.value)
+    return out, (b if b != 0xFFFFFFFF else None)

@@ -73,7 +73,7 @@ __device__ __forceinline__ uint32_t geom_quarter(uint64_t x)
 }
 
 struct bt_counters {
-	uint32_t mallocs, frees, nulls, bad, hits, puts, retired;
+	uint32_t mallocs, frees, nulls, bad, hits, puts, retired, refused;
 	unsigned long long fill, verify;
 };
 
@@ -229,6 +229,8 @@ __device__ __forceinline__ void bt_round(kma_heap *h, const bt_dev &w, const bt_
 			ct.fill += n;
 		} else {
 			ct.nulls++;
+			if (n > h->max_request)
+				ct.refused++;
 		}
 	}
 	__syncwarp(mask);
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(512, 2) k_bt_rounds(kma_heap *h, bt_dev w, uin
 		cc.hint[lane] = 0;
 	}
 	__syncwarp();
-	bt_counters ct = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+	bt_counters ct = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 	for (uint32_t r = 0; r <= w.rounds; r++) {
 		for (uint64_t base = 0; base < w.items; base += T) {
 			uint64_t g = base + tid;
@@ -280,10 +282,10 @@ __global__ void __launch_bounds__(512, 2) k_bt_rounds(kma_heap *h, bt_dev w, uin
 		}
 	}
 	const uint32_t mask = 0xffffffffu;
-	unsigned long long v[9] = {__reduce_add_sync(mask, ct.mallocs), __reduce_add_sync(mask, ct.frees),
-				   __reduce_add_sync(mask, ct.nulls), __reduce_add_sync(mask, ct.bad), 0, 0,
-				   __reduce_add_sync(mask, ct.hits), __reduce_add_sync(mask, ct.puts),
-				   __reduce_add_sync(mask, ct.retired)};
+	unsigned long long v[10] = {__reduce_add_sync(mask, ct.mallocs), __reduce_add_sync(mask, ct.frees),
+				    __reduce_add_sync(mask, ct.nulls), __reduce_add_sync(mask, ct.bad), 0, 0,
+				    __reduce_add_sync(mask, ct.hits), __reduce_add_sync(mask, ct.puts),
+				    __reduce_add_sync(mask, ct.retired), __reduce_add_sync(mask, ct.refused)};
 	unsigned long long f = ct.fill, vb = ct.verify;
 	for (int d = 16; d > 0; d >>= 1) {
 		f += __shfl_down_sync(mask, f, d);
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(512, 2) k_bt_rounds(kma_heap *h, bt_dev w, uin
 	v[4] = f;
 	v[5] = vb;
 	if (lane == 0)
-		for (int k = 0; k < 9; k++)
+		for (int k = 0; k < 10; k++)
 			if (v[k])
 				atomicAdd(&w.stats[k], v[k]);
 }
@@ -522,6 +524,7 @@ extern "C" int kma_batch_stats_get(kma_batch_t b, void *stream, kma_batch_stats 
 	out->cache_hits = v[6];
 	out->cache_puts = v[7];
 	out->retired = v[8];
+	out->refused = v[9];
 	return KMA_OK;
 }
 
@@ -573,6 +576,8 @@ extern "C" int kma_batch_autotune(const kma_batch_job *jobs, uint32_t njobs, uin
 				en->sb_size_log2 = sb_log2s[i];
 				en->block_dim = block_dims[j];
 				en->cache_depth = depths[k];
+				/* the largest size the jobs draw against the heap's largest request */
+				en->serves_all = 8u * BT_ZIPF_N <= h->hh.max_request;
 				rc = kma_batch_capture(b, block_dims[j], depths[k], st);
 				for (uint32_t w = 0; w < warmup && rc == KMA_OK; w++)
 					rc = kma_batch_launch(b, st);
@@ -598,7 +603,8 @@ extern "C" int kma_batch_autotune(const kma_batch_job *jobs, uint32_t njobs, uin
 				/* rank by successful calls per second: a NULL malloc is
 				 * cheap, and a configuration must not win by failing */
 				double good = (double)(en->stats.mallocs - en->stats.nulls + en->stats.frees) / en->ms;
-				if (en->stats.bad_tags == 0 && flags == 0 && (*best == 0xffffffffu || good > best_rate)) {
+				if (en->serves_all && en->stats.bad_tags == 0 && flags == 0 &&
+				    (*best == 0xffffffffu || good > best_rate)) {
 					*best = idx;
 					best_rate = good;
 				}

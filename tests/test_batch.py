@@ -43,8 +43,12 @@ def test_gpu_batch_run_invariants(sb_log2, depth):
         assert st["bad_tags"] == 0
         assert st["mallocs"] == items * 12
         assert st["frees"] == st["mallocs"] - st["nulls"]
-        if sb_log2 > 12:  # 4 KiB superblocks cannot hold 4088..4096-byte requests
-            assert st["nulls"] == 0
+        if sb_log2 > 12:
+            assert st["nulls"] == 0 and st["refused"] == 0
+        else:
+            # 4 KiB superblocks serve at most 4080 bytes: the jobs' 4088 and
+            # 4096-byte draws are refused, and those are all the NULLs here
+            assert st["refused"] == st["nulls"] > 0
         if depth:
             assert st["cache_hits"] > 0 and st["cache_puts"] >= st["cache_hits"]
         else:
@@ -77,9 +81,12 @@ def test_gpu_batch_autotune_reports_every_config():
     entries, best = autotune(SMALL_THREADS, list(range(len(SMALL_THREADS))), rounds=6,
                              heap_bytes=128 << 20, sb_log2s=(12, 14), block_dims=(128, 256),
                              depths=(0, 2), warmup=1, reps=1)
-    assert len(entries) == 8 and 0 <= best < 8
+    assert len(entries) == 8 and best is not None and 0 <= best < 8
     assert all(e["bad_tags"] == 0 and e["ms"] > 0 for e in entries)
     assert {(e["sb_size"], e["block_dim"], e["cache_depth"]) for e in entries} == \
         {(s, b, d) for s in (4096, 16384) for b in (128, 256) for d in (0, 2)}
-    rate = [(e["mallocs"] - e["nulls"] + e["frees"]) / e["ms"] for e in entries]
+    # a geometry that refuses sizes the jobs draw never wins, however fast
+    assert all(e["serves_all"] == (e["sb_size"] > 4096) for e in entries)
+    assert entries[best]["serves_all"] and entries[best]["refused"] == 0
+    rate = [(e["mallocs"] - e["nulls"] + e["frees"]) / e["ms"] if e["serves_all"] else 0 for e in entries]
     assert rate[best] == max(rate)
