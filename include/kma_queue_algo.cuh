@@ -1,5 +1,5 @@
 /*
- * kma_queue_algo.h -- the algorithms of the two lock-free FIFOs
+ * kma_queue_algo.cuh -- the algorithms of the two lock-free FIFOs
  * (kma_clqueue, clQueue.cl:27-118; kma_iqueue, clIndexedQueue.cl:44-290),
  * written once over an atomics policy so that the same text runs on the
  * GPU (kma_structs.cuh binds gpu-scope PTX atomics) and on host threads
@@ -33,8 +33,8 @@
  * Every wait is bounded by `limit` tries; expiry returns failure and the
  * caller records KMA_ERR_TIMEOUT.
  */
-#ifndef KMA_QUEUE_ALGO_H
-#define KMA_QUEUE_ALGO_H
+#ifndef KMA_QUEUE_ALGO_CUH
+#define KMA_QUEUE_ALGO_CUH
 
 #include <stdint.h>
 
@@ -236,4 +236,4 @@ KQ_FN uint32_t iq_dequeue_n(const Q &q, u64 *headw, uint32_t *out, uint32_t k, u
 
 } /* namespace kma_q */
 
-#endif /* KMA_QUEUE_ALGO_H */
+#endif /* KMA_QUEUE_ALGO_CUH */

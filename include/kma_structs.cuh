@@ -22,7 +22,7 @@
 #define KMA_STRUCTS_CUH
 
 #include "kma_device.cuh"
-#include "kma_queue_algo.h"
+#include "kma_queue_algo.cuh"
 
 #define KMA_STRUCT_SPIN (1u << 20)
 
@@ -73,7 +73,7 @@ __device__ __forceinline__ unsigned long long global_thread()
 	return blk * tpb + t;
 }
 
-/* The atomics policy of the queue algorithms (kma_queue_algo.h) on the
+/* The atomics policy of the queue algorithms (kma_queue_algo.cuh) on the
  * GPU: gpu-scope acquire/release PTX. */
 struct gpu_ops {
 	static __device__ __forceinline__ unsigned long long ld(unsigned long long *p) { return ld_acquire64(p); }
@@ -114,7 +114,7 @@ struct gpu_ops {
  * as the reference does (clQueue.cl:97), so a removed item keeps POISON in
  * its link until it is enqueued again.
  *
- * The algorithm is kma_queue_algo.h's (the text its host harness checks):
+ * The algorithm is kma_queue_algo.cuh's (the text its host harness checks):
  *   - enqueue exchanges the tail (always succeeds, one atomic), then links
  *     the previous tail item to the new one; the reference CASes the tail
  *     item's link in a retry loop and then the tail (clQueue.cl:40-75), so
@@ -359,7 +359,7 @@ __device__ __forceinline__ kma_clqueue_item *kma_clqueue_next(const kma_clqueue_
  * reference's: init makes `first` the dummy, dequeue returns the OLD dummy
  * (so `first` comes out first and the last item enqueued always stays
  * behind), NULL when only the dummy is left.  The algorithm is
- * kma_queue_algo.h's: enqueue exchanges the tail and links the previous
+ * kma_queue_algo.cuh's: enqueue exchanges the tail and links the previous
  * tail item (no retry loop, one atomic on the shared tail, where the
  * reference CASes the link and then the tail, clIndexedQueue.cl:132-196);
  * the warp forms append a warp's items as one chain and take a warp's

@@ -1,6 +1,6 @@
 /*
  * queue_harness.cpp -- TEST INFRASTRUCTURE: runs the queue algorithms of
- * include/kma_queue_algo.h (the text the GPU runs) on host threads, bound
+ * include/kma_queue_algo.cuh (the text the GPU runs) on host threads, bound
  * to GCC atomics, and checks what the device tests check at scale, plus
  * what a GPU run cannot provoke on purpose:
  *
@@ -38,7 +38,7 @@
 #include <thread>
 #include <vector>
 
-#include "kma_queue_algo.h"
+#include "kma_queue_algo.cuh"
 
 using kma_q::u64;
 

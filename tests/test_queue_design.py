@@ -1,4 +1,4 @@
-"""The queue algorithms of include/kma_queue_algo.h on host threads (no GPU).
+"""The queue algorithms of include/kma_queue_algo.cuh on host threads (no GPU).
 
 oracle/queue_harness runs the same algorithm text the GPU runs, bound to
 host atomics: producers append chains (a warp's items) and single items,
@@ -23,7 +23,7 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE = os.path.join(ROOT, "oracle")
 HARNESS = os.path.join(ORACLE, "queue_harness")
-ALGO = os.path.join(ROOT, "include", "kma_queue_algo.h")
+ALGO = os.path.join(ROOT, "include", "kma_queue_algo.cuh")
 
 # threads chains max_chain deq_batch delay_prob seed producers recycle
 CONFIGS = [
@@ -94,7 +94,7 @@ def test_harness_detects_planted_mistakes(harness, tmp_path, name):
     assert src.count(old) == 1, f"mutation site of {name} not found once"
     d = tmp_path / name
     d.mkdir()
-    (d / "kma_queue_algo.h").write_text(src.replace(old, new))
+    (d / "kma_queue_algo.cuh").write_text(src.replace(old, new))
     binary = str(d / "h")
     subprocess.run([os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-pthread", f"-I{d}", "-o", binary,
                     os.path.join(ORACLE, "queue_harness.cpp")], check=True)
