@@ -8,19 +8,21 @@
  * queue together.  The reference's edge file is not shipped, so callers
  * pass synthetic edges.
  *
- * Layout: heap blocks are 4-byte aligned, so a node (its links queue,
- * 16-byte aligned, then its tree node) sits at align16(block) inside a
- * 52-byte request -- the same size class as the reference's 40-byte
- * clGraph_node -- and a link (8-byte aligned queue link, then the sink's
- * offset from the first superblock / 4 as a u32) inside a 16-byte request,
- * the reference's clGraph_link size.  Serial runs therefore use the same
- * blocks as the reference.
+ * Layout: KMA heap blocks are 4-byte aligned, so a 40-byte node (its links
+ * queue, then its tree node) sits at align16(block) inside a 52-byte
+ * request -- the same size class as the reference's 40-byte clGraph_node;
+ * on the PMA heap the node is its 40-byte block.  A link (8-byte aligned
+ * queue link, then the sink's offset from the heap base / 8 as a u32) sits
+ * in a 16-byte request, the reference's clGraph_link size.  Serial runs
+ * therefore use the same blocks as the reference on either heap; heaps
+ * hold at most 32 GiB.
  */
 #ifndef KMA_GRAPH_H
 #define KMA_GRAPH_H
 
 #include <stdint.h>
 #include "kma.h"
+#include "kma_structs.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -52,6 +54,16 @@ uint64_t kma_graph_edge_mix(uint32_t source, uint32_t sink);
 int kma_graph_build(kma_heap_t h, const uint32_t *edges, uint64_t n, uint32_t threads, int free_after,
 		    kma_graph_stats *st, uint32_t *keys_out, int64_t *node_off, uint32_t *link_sinks,
 		    uint64_t *link_start);
+
+/* The same build (the same kernels, instantiated for the PMA heap) on PMA
+ * heap p, as the reference's driver runs tb_clTree.cl over pma.cl
+ * (test/tb_clTree.c:441-446): nodes and links are bump allocations and
+ * nothing is freed (a node that lost its add stays allocated; reset the
+ * PMA heap to reuse it).  node_off[i] is the node's own offset from the
+ * data base. */
+int kma_graph_build_pma(kma_pma_t p, const uint32_t *edges, uint64_t n, uint32_t threads,
+			kma_graph_stats *st, uint32_t *keys_out, int64_t *node_off, uint32_t *link_sinks,
+			uint64_t *link_start);
 
 #ifdef __cplusplus
 }

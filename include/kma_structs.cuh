@@ -132,7 +132,7 @@ struct gpu_ops {
  * Device pointers must be below 2^48 (the tag bits); enqueue refuses
  * others.
  */
-struct __align__(16) kma_clqueue {
+struct kma_clqueue {
 	unsigned long long head; /* {tag:16 | item ptr:48} */
 	unsigned long long tail; /* the last item's pointer, 0 when empty */
 };

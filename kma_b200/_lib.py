@@ -203,6 +203,8 @@ SIGNATURES = [
     ("kma_graph_edge_mix", c_uint64, [c_uint32, c_uint32]),
     ("kma_graph_build", c_int, [c_void_p, c_void_p, c_uint64, c_uint32, c_int, POINTER(KmaGraphStats),
                                 c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("kma_graph_build_pma", c_int, [c_void_p, c_void_p, c_uint64, c_uint32, POINTER(KmaGraphStats),
+                                    c_void_p, c_void_p, c_void_p, c_void_p]),
     # include/kma_serve.h
     ("kma_serve_create", c_int, [c_void_p, POINTER(KmaServeCfg), POINTER(c_void_p)]),
     ("kma_serve_destroy", c_int, [c_void_p]),

@@ -8,6 +8,10 @@
  * enqueue a freshly malloc'd link on the source's queue.  Every inserted
  * node is also recorded in a registry array, so the walk and the teardown
  * run one thread per node.
+ *
+ * Every kernel is a template on the heap backend (kma_backend.cuh), as the
+ * reference's driver builds the same tb_clTree.cl over kma.cl or pma.cl
+ * (test/tb_clTree.c:441-446, 478-480).
  */
 #include <string.h>
 #include <stdlib.h>
@@ -17,16 +21,32 @@
 
 #include "kma_internal.h"
 #include "kma_graph.h"
+#include "kma_structs.h"
 #include "kma_structs.cuh"
+#include "kma_backend.cuh"
 
-#define GR_NODE_REQ 52u /* 40-byte node at align16(block): the reference's 40-byte class */
 #define GR_LINK_REQ 16u /* the reference's clGraph_link size */
 
 namespace {
 
-struct __align__(16) gr_node {
-	kma_clqueue links;     /* 16-byte aligned for the 16-byte CAS */
+/* 40 bytes, the reference's clGraph_node size (tb_clTree.h) */
+struct gr_node {
+	kma_clqueue links;
 	kma_cltree_node tree;  /* key, state, left, right */
+};
+
+/* Where a node sits in its block.  KMA blocks are only 4-byte aligned, so
+ * the node goes to align16(block) inside a 52-byte request, the same size
+ * class as the reference's 40-byte request; PMA blocks of this build are
+ * 8-byte aligned (40- and 16-byte requests from an aligned base), so the
+ * node is the block and the request is the reference's own 40 bytes:
+ * either way serial builds use the reference's blocks. */
+template <class B> struct gr_layout;
+template <> struct gr_layout<kma_backend_kma> {
+	static constexpr uint32_t node_req = 52, node_align = 16;
+};
+template <> struct gr_layout<kma_backend_pma> {
+	static constexpr uint32_t node_req = 40, node_align = 8;
 };
 
 __host__ __device__ __forceinline__ uint64_t gr_mix(uint32_t a, uint32_t b)
@@ -42,8 +62,9 @@ __device__ __forceinline__ gr_node *gr_of_tree(kma_cltree_node *t)
 	return reinterpret_cast<gr_node *>(reinterpret_cast<unsigned char *>(t) - offsetof(gr_node, tree));
 }
 
+template <class B>
 struct gr_dev {
-	kma_heap *h;
+	typename B::heap *h;
 	kma_cltree *tree;
 	gr_node **reg;               /* [cap] inserted nodes */
 	unsigned long long *nreg;
@@ -53,18 +74,20 @@ struct gr_dev {
 
 /* clGraph_node_ensure (tb_clTree.cl:12-38); NULL when the heap is out of
  * blocks (the reference retries forever there) */
-__device__ gr_node *gr_ensure(const gr_dev &g, uint32_t key, unsigned long long &lost, unsigned long long &nulls)
+template <class B>
+__device__ gr_node *gr_ensure(const gr_dev<B> &g, uint32_t key, unsigned long long &lost, unsigned long long &nulls)
 {
 	for (int tries = 0; tries < 1 << 20; tries++) {
 		kma_cltree_node *t = kma_cltree_get(g.tree, key);
 		if (t)
 			return gr_of_tree(t);
-		void *b = kma_malloc(g.h, GR_NODE_REQ);
+		void *b = B::alloc(g.h, gr_layout<B>::node_req);
 		if (!b) {
 			nulls++;
 			return nullptr;
 		}
-		gr_node *n = reinterpret_cast<gr_node *>(((uintptr_t)b + 15) & ~(uintptr_t)15);
+		const uintptr_t al = gr_layout<B>::node_align - 1;
+		gr_node *n = reinterpret_cast<gr_node *>(((uintptr_t)b + al) & ~al);
 		n->tree.key = key;
 		kma_clqueue_init(&n->links);
 		__threadfence();
@@ -73,7 +96,7 @@ __device__ gr_node *gr_ensure(const gr_dev &g, uint32_t key, unsigned long long 
 			g.reg[i] = n;
 			return n;
 		}
-		kma_free(g.h, b);
+		B::release(g.h, b);
 		lost++;
 	}
 	atomicOr(g.qerr, KMA_ERR_TIMEOUT);
@@ -81,7 +104,8 @@ __device__ gr_node *gr_ensure(const gr_dev &g, uint32_t key, unsigned long long 
 }
 
 /* clTree_test (tb_clTree.cl:40-85) */
-__global__ void k_gr_build(gr_dev g, const uint32_t *edges, uint64_t n)
+template <class B>
+__global__ void k_gr_build(gr_dev<B> g, const uint32_t *edges, uint64_t n)
 {
 	uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
 	unsigned long long lost = 0, nulls = 0;
@@ -90,13 +114,13 @@ __global__ void k_gr_build(gr_dev g, const uint32_t *edges, uint64_t n)
 		gr_node *snk = gr_ensure(g, edges[2 * i + 1], lost, nulls);
 		if (!src || !snk)
 			continue;
-		void *b = kma_malloc(g.h, GR_LINK_REQ);
+		void *b = B::alloc(g.h, GR_LINK_REQ);
 		if (!b) {
 			nulls++;
 			continue;
 		}
 		unsigned char *item = reinterpret_cast<unsigned char *>(((uintptr_t)b + 7) & ~(uintptr_t)7);
-		*reinterpret_cast<uint32_t *>(item + 8) = (uint32_t)(((unsigned char *)snk - g.h->sb_base) >> 4);
+		*reinterpret_cast<uint32_t *>(item + 8) = (uint32_t)(((unsigned char *)snk - B::base(g.h)) >> 3);
 		__threadfence();
 		kma_clqueue_enqueue(&src->links, reinterpret_cast<kma_clqueue_item *>(item), g.qerr);
 	}
@@ -106,16 +130,18 @@ __global__ void k_gr_build(gr_dev g, const uint32_t *edges, uint64_t n)
 		atomicAdd(&g.acc[1], nulls);
 }
 
-__device__ __forceinline__ uint32_t gr_sink_key(const gr_dev &g, const kma_clqueue_item *it)
+template <class B>
+__device__ __forceinline__ uint32_t gr_sink_key(const gr_dev<B> &g, const kma_clqueue_item *it)
 {
-	uint32_t off16 = *reinterpret_cast<const uint32_t *>(reinterpret_cast<const unsigned char *>(it) + 8);
-	const gr_node *s = reinterpret_cast<const gr_node *>(g.h->sb_base + ((size_t)off16 << 4));
+	uint32_t off8 = *reinterpret_cast<const uint32_t *>(reinterpret_cast<const unsigned char *>(it) + 8);
+	const gr_node *s = reinterpret_cast<const gr_node *>(B::base(g.h) + ((size_t)off8 << 3));
 	return s->tree.key;
 }
 
 /* per node: links in queue order -> count, edge hashes; optionally the
  * sinks at out[start[i] ...] */
-__global__ void k_gr_walk(gr_dev g, uint64_t nodes, unsigned long long *counts, const uint64_t *start,
+template <class B>
+__global__ void k_gr_walk(gr_dev<B> g, uint64_t nodes, unsigned long long *counts, const uint64_t *start,
 		uint32_t *sinks, unsigned long long *sums /* links, xor, sum */)
 {
 	uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -144,14 +170,26 @@ __global__ void k_gr_walk(gr_dev g, uint64_t nodes, unsigned long long *counts, 
 		atomicAdd(&sums[2], s);
 }
 
-__global__ void k_gr_export(gr_dev g, uint64_t nodes, uint32_t *keys, long long *offs)
+/* offset of the block that holds node nd (PMA: of the node itself, its
+ * blocks have no recorded start) */
+__device__ __forceinline__ long long gr_block_off(kma_heap *h, const gr_node *nd)
+{
+	return (long long)((const unsigned char *)kma_block_of(h, nd) - h->sb_base);
+}
+__device__ __forceinline__ long long gr_block_off(kma_pma *p, const gr_node *nd)
+{
+	return (long long)((const unsigned char *)nd - p->base);
+}
+
+template <class B>
+__global__ void k_gr_export(gr_dev<B> g, uint64_t nodes, uint32_t *keys, long long *offs)
 {
 	uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= nodes)
 		return;
 	const gr_node *nd = g.reg[i];
 	keys[i] = nd->tree.key;
-	offs[i] = (long long)((const unsigned char *)kma_block_of(g.h, nd) - g.h->sb_base);
+	offs[i] = gr_block_off(g.h, nd);
 }
 
 /* in-order walk with an explicit stack: strictly increasing keys? */
@@ -183,7 +221,8 @@ __global__ void k_gr_sorted(const kma_cltree *t, unsigned long long *stack, uint
 }
 
 /* teardown: every node frees its links, then itself */
-__global__ void k_gr_free(gr_dev g, uint64_t nodes)
+template <class B>
+__global__ void k_gr_free(gr_dev<B> g, uint64_t nodes)
 {
 	uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= nodes)
@@ -193,26 +232,30 @@ __global__ void k_gr_free(gr_dev g, uint64_t nodes)
 		kma_clqueue_item *it = kma_clqueue_dequeue(&nd->links, g.qerr);
 		if (!it)
 			break;
-		kma_free(g.h, kma_block_of(g.h, it));
+		B::release(g.h, it);
 	}
-	kma_free(g.h, kma_block_of(g.h, nd));
+	B::release(g.h, nd);
 }
 
 } /* namespace */
 
 extern "C" uint64_t kma_graph_edge_mix(uint32_t source, uint32_t sink) { return gr_mix(source, sink); }
 
-extern "C" int kma_graph_build(kma_heap_t h, const uint32_t *edges, uint64_t n, uint32_t threads, int free_after,
-		kma_graph_stats *st, uint32_t *keys_out, int64_t *node_off, uint32_t *link_sinks,
-		uint64_t *link_start)
+namespace {
+/* The build on heap dh (device header) of either backend; region_bytes:
+ * the heap's data bytes (sink offsets are 32-bit multiples of 8 bytes). */
+template <class B>
+int graph_build(typename B::heap *dh, int device, uint64_t region_bytes, const uint32_t *edges, uint64_t n,
+		uint32_t threads, int free_after, kma_graph_stats *st, uint32_t *keys_out, int64_t *node_off,
+		uint32_t *link_sinks, uint64_t *link_start)
 {
-	if (!h || !edges || !st || n == 0 || n > (1ull << 30) || threads == 0)
+	if (!dh || !edges || !st || n == 0 || n > (1ull << 30) || threads == 0)
 		return KMA_EINVAL;
-	if (h->hh.region_bytes > (1ull << 36)) /* sink offsets are 32-bit multiples of 16 bytes */
+	if (region_bytes > (1ull << 35))
 		return KMA_EINVAL;
 	if (keys_out && (!node_off || !link_sinks || !link_start))
 		return KMA_EINVAL;
-	kma_device_guard gd(h->device);
+	kma_device_guard gd(device);
 	memset(st, 0, sizeof(*st));
 	uint64_t cap = 2 * n;
 	void *mem = NULL;
@@ -226,8 +269,8 @@ extern "C" int kma_graph_build(kma_heap_t h, const uint32_t *edges, uint64_t n, 
 	}
 	unsigned char *m = (unsigned char *)mem;
 	int rc = KMA_OK;
-	gr_dev g;
-	g.h = h->dh;
+	gr_dev<B> g;
+	g.h = dh;
 	g.tree = (kma_cltree *)(m + o_tree);
 	g.reg = (gr_node **)(m + o_reg);
 	g.nreg = (unsigned long long *)(m + o_nreg);
@@ -244,7 +287,7 @@ extern "C" int kma_graph_build(kma_heap_t h, const uint32_t *edges, uint64_t n, 
 		uint32_t bd = threads < 256 ? threads : 256;
 		uint32_t nb = (threads + bd - 1) / bd;
 		cudaEventRecord(e0);
-		k_gr_build<<<nb, bd>>>(g, (const uint32_t *)(m + o_edges), n);
+		k_gr_build<B><<<nb, bd>>>(g, (const uint32_t *)(m + o_edges), n);
 		cudaEventRecord(e1);
 		if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
 			rc = KMA_ECUDA;
@@ -258,7 +301,7 @@ extern "C" int kma_graph_build(kma_heap_t h, const uint32_t *edges, uint64_t n, 
 	uint32_t gb = (uint32_t)((nodes + 255) / 256);
 	if (rc == KMA_OK && nodes) {
 		unsigned long long *cnt = (unsigned long long *)(m + o_cnt);
-		k_gr_walk<<<gb, 256>>>(g, nodes, keys_out ? cnt : NULL, NULL, NULL, sums);
+		k_gr_walk<B><<<gb, 256>>>(g, nodes, keys_out ? cnt : NULL, NULL, NULL, sums);
 		k_gr_sorted<<<1, 1>>>(g.tree, (unsigned long long *)(m + o_stack), 1 << 20, sums + 4);
 		if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
 			rc = KMA_ECUDA;
@@ -276,7 +319,7 @@ extern "C" int kma_graph_build(kma_heap_t h, const uint32_t *edges, uint64_t n, 
 			std::vector<unsigned long long> c(nodes);
 			std::vector<uint32_t> k(nodes);
 			std::vector<long long> o(nodes);
-			k_gr_export<<<gb, 256>>>(g, nodes, (uint32_t *)(m + o_keys), (long long *)(m + o_offs));
+			k_gr_export<B><<<gb, 256>>>(g, nodes, (uint32_t *)(m + o_keys), (long long *)(m + o_offs));
 			if (cudaDeviceSynchronize() != cudaSuccess ||
 			    cudaMemcpy(c.data(), cnt, nodes * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
 			    cudaMemcpy(k.data(), m + o_keys, nodes * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
@@ -289,8 +332,8 @@ extern "C" int kma_graph_build(kma_heap_t h, const uint32_t *edges, uint64_t n, 
 				if (cudaMemcpy(m + o_start, start.data(), (nodes + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess)
 					rc = KMA_ECUDA;
 				cudaMemset(sums, 0, 24);
-				k_gr_walk<<<gb, 256>>>(g, nodes, NULL, (const uint64_t *)(m + o_start), (uint32_t *)(m + o_sinks),
-						      sums);
+				k_gr_walk<B><<<gb, 256>>>(g, nodes, NULL, (const uint64_t *)(m + o_start),
+							 (uint32_t *)(m + o_sinks), sums);
 				std::vector<uint32_t> sk(start[nodes] ? start[nodes] : 1);
 				if (rc == KMA_OK && (cudaDeviceSynchronize() != cudaSuccess ||
 						     cudaMemcpy(sk.data(), m + o_sinks, start[nodes] * 4,
@@ -317,7 +360,7 @@ extern "C" int kma_graph_build(kma_heap_t h, const uint32_t *edges, uint64_t n, 
 		}
 	}
 	if (rc == KMA_OK && free_after && nodes) {
-		k_gr_free<<<gb, 256>>>(g, nodes);
+		k_gr_free<B><<<gb, 256>>>(g, nodes);
 		if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
 			rc = KMA_ECUDA;
 	}
@@ -331,4 +374,25 @@ extern "C" int kma_graph_build(kma_heap_t h, const uint32_t *edges, uint64_t n, 
 	cudaEventDestroy(e1);
 	cudaFree(mem);
 	return rc;
+}
+} /* namespace */
+
+extern "C" int kma_graph_build(kma_heap_t h, const uint32_t *edges, uint64_t n, uint32_t threads, int free_after,
+		kma_graph_stats *st, uint32_t *keys_out, int64_t *node_off, uint32_t *link_sinks,
+		uint64_t *link_start)
+{
+	if (!h)
+		return KMA_EINVAL;
+	return graph_build<kma_backend_kma>(h->dh, h->device, h->hh.region_bytes, edges, n, threads, free_after, st,
+					    keys_out, node_off, link_sinks, link_start);
+}
+
+extern "C" int kma_graph_build_pma(kma_pma_t p, const uint32_t *edges, uint64_t n, uint32_t threads,
+		kma_graph_stats *st, uint32_t *keys_out, int64_t *node_off, uint32_t *link_sinks,
+		uint64_t *link_start)
+{
+	if (!p)
+		return KMA_EINVAL;
+	return graph_build<kma_backend_pma>(p->dp, p->device, p->bytes, edges, n, threads, 0, st, keys_out, node_off,
+					    link_sinks, link_start);
 }

@@ -12,6 +12,7 @@
 #include <stdlib.h>
 #include <vector>
 #include "kma_internal.h"
+#include "kma_backend.cuh"
 
 /* ------------------------------------------------------------------ */
 /* class tables                                                        */
@@ -161,30 +162,6 @@ __global__ void kma_k_gather_bitmaps(kma_heap *h, uint32_t *dst, uint32_t words)
 	for (uint64_t i = tid; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
 		uint32_t s = (uint32_t)(i / words), k = (uint32_t)(i % words);
 		dst[i] = *kma_detail::bitmap_word(h, kma_detail::sb_addr(h, s), k);
-	}
-}
-
-/* One thread replays the op stream (see kma_replay in kma.h). */
-__global__ void kma_k_replay(kma_heap *h, const int64_t *ops, int64_t n, int64_t *out, int mode)
-{
-	if (blockIdx.x != 0 || threadIdx.x != 0)
-		return;
-	for (int64_t i = 0; i < n; i++) {
-		int64_t kind = ops[2 * i], arg = ops[2 * i + 1];
-		if (kind == 0) {
-			size_t sz = arg < 0 ? (size_t)-1 : (size_t)arg;
-			void *p = mode == KMA_MODE_WARP ? kma_malloc_warp(h, sz) : kma_malloc(h, sz);
-			out[i] = p ? (int64_t)((unsigned char *)p - h->sb_base) : -1;
-		} else {
-			void *q = NULL;
-			if (arg >= 0 && arg < i && out[arg] >= 0)
-				q = h->sb_base + out[arg];
-			if (mode == KMA_MODE_WARP)
-				kma_free_warp(h, q);
-			else
-				kma_free(h, q);
-			out[i] = 0;
-		}
 	}
 }
 
@@ -495,7 +472,7 @@ extern "C" int kma_replay(kma_heap_t h, const int64_t *ops, int64_t n, int64_t *
 	kma_device_guard g(h->device);
 	if (n == 0)
 		return KMA_OK;
-	kma_k_replay<<<1, 1, 0, kma_stream(stream)>>>(h->dh, ops, n, out, mode);
+	kma_k_heap_replay<kma_backend_kma><<<1, 1, 0, kma_stream(stream)>>>(h->dh, ops, n, out, mode == KMA_MODE_WARP);
 	KMA_CUDA(cudaGetLastError());
 	return KMA_OK;
 }

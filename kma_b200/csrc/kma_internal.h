@@ -16,6 +16,15 @@ struct kma_heap_s {
 	kma_heap hh;         /* host copy of the header's geometry */
 };
 
+struct kma_pma;
+struct kma_pma_s {
+	int device;
+	void *mem;
+	kma_pma *dp;         /* device header */
+	unsigned char *base; /* data base */
+	uint64_t bytes;      /* data bytes */
+};
+
 #define KMA_DEFAULT_SPIN (1u << 22)
 
 static inline cudaStream_t kma_stream(void *s) { return (cudaStream_t)s; }

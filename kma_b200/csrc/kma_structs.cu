@@ -13,14 +13,8 @@
 #include "kma_internal.h"
 #include "kma_structs.h"
 #include "kma_structs.cuh"
+#include "kma_backend.cuh"
 
-struct kma_pma_s {
-	int device;
-	void *mem;
-	kma_pma *dp;
-	unsigned char *base;
-	uint64_t bytes; /* data bytes */
-};
 struct kma_clqueue_s {
 	int device;
 	kma_clqueue *dq;
@@ -157,20 +151,6 @@ extern "C" int kma_pma_head(kma_pma_t p, void *stream, uint64_t *head)
 }
 
 namespace {
-__global__ void k_pma_replay(kma_pma *p, const int64_t *ops, int64_t n, int64_t *out)
-{
-	for (int64_t i = 0; i < n; i++) {
-		int64_t kind = ops[2 * i], arg = ops[2 * i + 1];
-		if (kind == 0) {
-			void *r = kma_pma_malloc(p, (size_t)arg);
-			out[i] = r ? (int64_t)((unsigned char *)r - p->base) : -1;
-		} else {
-			void *q = (arg >= 0 && arg < i && out[arg] >= 0) ? p->base + out[arg] : NULL;
-			kma_pma_free(p, q);
-			out[i] = 0;
-		}
-	}
-}
 } /* namespace */
 
 /* run a one-thread replay kernel over host op/out arrays */
@@ -201,7 +181,7 @@ extern "C" int kma_pma_replay_host(kma_pma_t p, const int64_t *ops, int64_t n, i
 		return KMA_EINVAL;
 	kma_device_guard g(p->device);
 	return replay_host(n, ops, out, [&](const int64_t *dops, int64_t *dout) {
-		k_pma_replay<<<1, 1>>>(p->dp, dops, n, dout);
+		kma_k_heap_replay<kma_backend_pma><<<1, 1>>>(p->dp, dops, n, dout, 0);
 		return KMA_OK;
 	});
 }

@@ -28,8 +28,10 @@ def synth_edges(seed: int, n_edges: int, n_vertices: int, skew: float = 1.1) -> 
     return np.stack([keys[src], keys[dst]], axis=1).astype(np.uint32)
 
 
-def build(heap: Heap, edges: np.ndarray, threads: int, free_after: bool = True, export: bool = False):
-    """Run the build; returns (stats, export) where export is None or
+def build(heap, edges: np.ndarray, threads: int, free_after: bool = True, export: bool = False):
+    """Run the build on a Heap, or on a structs.Pma (the same kernels
+    instantiated for the bump heap, which frees nothing: free_after does
+    not apply); returns (stats, export) where export is None or
     (keys, node_offsets, link_sinks, link_start) in key order."""
     edges = np.ascontiguousarray(edges, np.uint32).reshape(-1, 2)
     n = len(edges)
@@ -42,8 +44,12 @@ def build(heap: Heap, edges: np.ndarray, threads: int, free_after: bool = True, 
         ptrs = (keys.ctypes.data, offs.ctypes.data, sinks.ctypes.data, start.ctypes.data)
     else:
         ptrs = (None, None, None, None)
-    check(lib().kma_graph_build(heap.handle, edges.ctypes.data, n, threads, int(free_after), byref(st), *ptrs),
-          "kma_graph_build")
+    if isinstance(heap, Heap):
+        check(lib().kma_graph_build(heap.handle, edges.ctypes.data, n, threads, int(free_after), byref(st),
+                                    *ptrs), "kma_graph_build")
+    else:
+        check(lib().kma_graph_build_pma(heap.handle, edges.ctypes.data, n, threads, byref(st), *ptrs),
+              "kma_graph_build_pma")
     stats = {k: getattr(st, k) for k, _ in KmaGraphStats._fields_ if k != "pad"}
     if not export:
         return stats, None

@@ -1,13 +1,17 @@
 /*
- * ref_pma_unit.c -- the reference's poor man's allocator (pma.cl) and the
- * array list over it (clQueue.cl + clArrayList.cl), compiled unmodified
- * where they lie.  TEST INFRASTRUCTURE ONLY (oracle/_ref/).
+ * ref_pma_unit.c -- the reference's poor man's allocator (pma.cl), the
+ * array list over it (clQueue.cl + clArrayList.cl) and the tree driver's
+ * graph build over it (clTree.cl + test/tb_clTree.cl, which the reference
+ * runs on pma.cl too, test/tb_clTree.c:478-480), compiled unmodified where
+ * they lie.  TEST INFRASTRUCTURE ONLY (oracle/_ref/).
  */
 #include "ref_shim.h"
 
 #include "pma.cl"
 #include "clQueue.cl"
 #include "clArrayList.cl"
+#include "clTree.cl"
+#include "test/tb_clTree.cl"
 
 #undef malloc
 #undef free
@@ -78,4 +82,15 @@ void oref_pma_replay(void *p, const int64_t *ops, int64_t n, int64_t *out)
 			out[i] = 0;
 		}
 	}
+}
+
+/* ---- graph build (test/tb_clTree.cl:12-85) over pma.cl, one work-item -- */
+void *oref_pma_heap(void *p) { return ((struct oref_pma *)p)->heap; }
+uint64_t oref_pma_data_base(void *p) { return (uint64_t)(uintptr_t)((struct oref_pma *)p)->heap->base; }
+void oref_pma_graph_build_serial(void *p, void *tree_root_word, const uint32_t *edges, uint32_t items)
+{
+	oref_wi.dim = 1;
+	oref_wi.gid[0] = 0;
+	oref_wi.gsize[0] = 1;
+	clTree_test(((struct oref_pma *)p)->heap, tree_root_word, (struct clTree_link *)edges, items);
 }

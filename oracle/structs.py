@@ -73,6 +73,8 @@ def _pma_lib() -> ctypes.CDLL:
             ("oref_pma_create", c_void_p, [c_uint64]), ("oref_pma_destroy", None, [c_void_p]),
             ("oref_pma_replay", None, [c_void_p, c_void_p, c_int64, c_void_p]),
             ("oref_pma_head", c_uint32, [c_void_p]), ("oref_pma_header_bytes", c_uint32, []),
+            ("oref_pma_data_base", c_uint64, [c_void_p]),
+            ("oref_pma_graph_build_serial", None, [c_void_p, c_void_p, c_void_p, c_uint32]),
         ]:
             f = getattr(L, name)
             f.restype = res
@@ -234,6 +236,33 @@ def pma_replay(nbytes: int, ops: np.ndarray):
     return out
 
 
+def _graph_walk(root_addr: int, base: int):
+    """In-order walk of a reference graph: (keys, node offsets from `base`,
+    link sinks, link start), nodes in key order, each node's links in queue
+    order.  clGraph_node = {clTree_node (key, left, right), clQueue links};
+    clGraph_link = {next, sink}."""
+    u64 = lambda a: ctypes.c_uint64.from_address(a).value  # noqa: E731
+    u32 = lambda a: ctypes.c_uint32.from_address(a).value  # noqa: E731
+    keys, offs, sinks, start = [], [], [], []
+    stack, cur = [], u64(root_addr)
+    while cur or stack:
+        while cur:
+            stack.append(cur)
+            cur = u64(cur + 8)
+        cur = stack.pop()
+        keys.append(u32(cur))
+        offs.append(cur - base)
+        start.append(len(sinks))
+        link = u64(cur + 24)  # links.head
+        while link:
+            sinks.append(u32(u64(link + 8)))
+            link = u64(link)
+        cur = u64(cur + 16)
+    start.append(len(sinks))
+    return (np.array(keys, np.int64), np.array(offs, np.int64), np.array(sinks, np.int64),
+            np.array(start, np.int64))
+
+
 def graph_build(sblocks: int, edges: np.ndarray):
     """tb_clTree.cl clTree_test run by one work-item over a fresh reference
     KMA heap of `sblocks` 4 KiB superblocks: (keys, node offsets from the
@@ -245,28 +274,26 @@ def graph_build(sblocks: int, edges: np.ndarray):
     h = L.oref_heap_create(sblocks)
     base = L.oref_heap_sb_base(h)
     t = L.oref_tree_create()
-    u64 = lambda a: ctypes.c_uint64.from_address(a).value  # noqa: E731
-    u32 = lambda a: ctypes.c_uint32.from_address(a).value  # noqa: E731
     try:
         L.oref_graph_build_serial(h, t, edges.ctypes.data, len(edges))
-        keys, offs, sinks, start = [], [], [], []
-        stack, cur = [], u64(t)
-        while cur or stack:  # clGraph_node = {clTree_node (key, left, right), clqueue links}
-            while cur:
-                stack.append(cur)
-                cur = u64(cur + 8)
-            cur = stack.pop()
-            keys.append(u32(cur))
-            offs.append(cur - base)
-            start.append(len(sinks))
-            link = u64(cur + 24)  # links.head; clGraph_link = {next, sink}
-            while link:
-                sinks.append(u32(u64(link + 8)))
-                link = u64(link)
-            cur = u64(cur + 16)
-        start.append(len(sinks))
+        return _graph_walk(t, base)
     finally:
         L.oref_tree_destroy(t)
         L.oref_heap_destroy(h)
-    return (np.array(keys, np.int64), np.array(offs, np.int64), np.array(sinks, np.int64),
-            np.array(start, np.int64))
+
+
+def graph_build_pma(nbytes: int, edges: np.ndarray):
+    """The same build over the reference's pma.cl (as test/tb_clTree.c:478-480
+    runs it) on a fresh PMA heap of `nbytes` data bytes; node offsets are
+    from the heap's data base."""
+    L, P = _cl_lib(), _pma_lib()
+    edges = np.ascontiguousarray(edges, np.uint32).reshape(-1, 2)
+    p = P.oref_pma_create(nbytes)
+    base = P.oref_pma_data_base(p)
+    t = L.oref_tree_create()
+    try:
+        P.oref_pma_graph_build_serial(p, t, edges.ctypes.data, len(edges))
+        return _graph_walk(t, base)
+    finally:
+        L.oref_tree_destroy(t)
+        P.oref_pma_destroy(p)

@@ -39,6 +39,9 @@ PMA_EDGE = [4096, 1000]
 GRAPH = [(61, 64, 400, 60), (62, 256, 3000, 700)]          # (seed, sblocks, edges, vertices)
 
 
+GRAPH_PMA_BYTES = 2097152
+
+
 def graph_edges(seed: int, n_edges: int, n_vertices: int) -> np.ndarray:
     """Synthetic edges (the reference's edge file is not shipped): Zipf(1.1)
     vertex ranks mapped to distinct random u32 keys."""
@@ -89,6 +92,12 @@ def cases() -> dict:
         out[f"graph_{seed}_edges"], out[f"graph_{seed}_keys"] = e.astype(np.int64), k
         out[f"graph_{seed}_offs"], out[f"graph_{seed}_sinks"], out[f"graph_{seed}_start"] = o, sk, st
         out[f"graph_{seed}_cfg"] = np.array([sblocks])
+        # the same build over the reference's pma.cl (test/tb_clTree.c:478-480,
+        # its 2 MiB PMA heap): the same nodes and links, bump-allocated
+        k, o, sk, st = structs.graph_build_pma(GRAPH_PMA_BYTES, e)
+        out[f"graphpma_{seed}_keys"], out[f"graphpma_{seed}_offs"] = k, o
+        out[f"graphpma_{seed}_sinks"], out[f"graphpma_{seed}_start"] = sk, st
+        out[f"graphpma_{seed}_cfg"] = np.array([GRAPH_PMA_BYTES])
     return out
 
 
