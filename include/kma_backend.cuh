@@ -22,6 +22,10 @@
  *                        frees by the object's address); PMA: nothing
  *   alloc_warp / release_warp   the warp-collaborative forms (any subset of
  *                        a warp may call them)
+ *   free_block / free_block_warp   free, for callers holding exactly the
+ *                        pointer alloc returned (no search for the block)
+ *   no_request           the size a lane passes to alloc_warp when it wants
+ *                        nothing (its result is NULL or to be ignored)
  *   base(h)              the address heap offsets are counted from
  */
 #ifndef KMA_BACKEND_CUH
@@ -41,6 +45,9 @@ struct kma_backend_kma {
 	static __device__ __forceinline__ void release(heap *h, void *p) { kma_free(h, block(h, p)); }
 	static __device__ __forceinline__ void *alloc_warp(heap *h, size_t n) { return kma_malloc_warp(h, n); }
 	static __device__ __forceinline__ void release_warp(heap *h, void *p) { kma_free_warp(h, block(h, p)); }
+	static __device__ __forceinline__ void free_block(heap *h, void *p) { kma_free(h, p); }
+	static __device__ __forceinline__ void free_block_warp(heap *h, void *p) { kma_free_warp(h, p); }
+	static constexpr size_t no_request = ~(size_t)0; /* above every class: NULL at once */
 	static __device__ __forceinline__ unsigned char *base(const heap *h) { return h->sb_base; }
 	/* the largest request served (SB - 16, kma.cl:126) */
 	static __device__ __forceinline__ size_t max_request(const heap *h) { return h->max_request; }
@@ -65,6 +72,9 @@ struct kma_backend_pma {
 	static __device__ __forceinline__ void release(heap *h, void *p) { kma_pma_free(h, p); }
 	static __device__ __forceinline__ void *alloc_warp(heap *h, size_t n) { return kma_pma_malloc_warp(h, n); }
 	static __device__ __forceinline__ void release_warp(heap *h, void *p) { kma_pma_free(h, p); }
+	static __device__ __forceinline__ void free_block(heap *h, void *p) { kma_pma_free(h, p); }
+	static __device__ __forceinline__ void free_block_warp(heap *h, void *p) { kma_pma_free(h, p); }
+	static constexpr size_t no_request = 0; /* adds nothing to the warp's bump */
 	static __device__ __forceinline__ unsigned char *base(const heap *h) { return h->base; }
 	static __device__ __forceinline__ size_t max_request(const heap *) { return ~(size_t)0; }
 };
@@ -103,9 +113,9 @@ __global__ void kma_k_heap_replay(typename B::heap *h, const int64_t *ops, int64
 		} else {
 			void *q = (arg >= 0 && arg < i && out[arg] >= 0) ? B::base(h) + out[arg] : nullptr;
 			if (warp)
-				B::release_warp(h, q);
+				B::free_block_warp(h, q);
 			else
-				B::release(h, q);
+				B::free_block(h, q);
 			out[i] = 0;
 		}
 	}

@@ -22,6 +22,7 @@
 
 #include <stdint.h>
 #include "kma.h"
+#include "kma_structs.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -48,9 +49,22 @@ typedef struct kma_batch_stats {
 
 #define KMA_BATCH_MAX_CACHE 8
 
-/* A batch of `njobs` jobs (<= 4096) running `rounds` rounds on heap h. */
+/* A batch of `njobs` jobs (<= 4096) running `rounds` rounds on heap h
+ * (at most 16 GiB). */
 int kma_batch_create(kma_heap_t h, const kma_batch_job *jobs, uint32_t njobs, uint32_t rounds,
 		     kma_batch_t *out);
+/* The same batch on the PMA heap p (at most 32 GiB): the same kernel,
+ * compiled for the bump heap (kma_backend.cuh), as the reference runs its
+ * drivers over pma.cl for comparison (test/tb_clArrayList.c:221-223).
+ * Frees do nothing there, so the jobs need the sum of all their requests;
+ * a run resets p first.  Cache depth must be 0. */
+int kma_batch_create_pma(kma_pma_t p, const kma_batch_job *jobs, uint32_t njobs, uint32_t rounds,
+			 kma_batch_t *out);
+/* Call style of later runs and captures: KMA_MODE_WARP (the default:
+ * kma_malloc_warp / kma_free_warp, and the warp cache) or KMA_MODE_PLAIN
+ * (every thread calls kma_malloc / kma_free itself, the reference's
+ * per-work-item calls, kma.cl:279-373; cache depth must be 0). */
+int kma_batch_set_mode(kma_batch_t b, int mode);
 int kma_batch_destroy(kma_batch_t b);
 uint64_t kma_batch_items(kma_batch_t b);
 

@@ -190,6 +190,8 @@ SIGNATURES = [
                                 POINTER(KmaC3TreeStats)]),
     # include/kma_batch.h
     ("kma_batch_create", c_int, [c_void_p, POINTER(KmaBatchJob), c_uint32, c_uint32, POINTER(c_void_p)]),
+    ("kma_batch_create_pma", c_int, [c_void_p, POINTER(KmaBatchJob), c_uint32, c_uint32, POINTER(c_void_p)]),
+    ("kma_batch_set_mode", c_int, [c_void_p, c_int]),
     ("kma_batch_destroy", c_int, [c_void_p]),
     ("kma_batch_items", c_uint64, [c_void_p]),
     ("kma_batch_run", c_int, [c_void_p, c_uint32, c_uint32, c_void_p]),

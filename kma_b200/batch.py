@@ -37,14 +37,24 @@ def _stats(st: KmaBatchStats) -> dict:
 
 
 class Batch:
-    def __init__(self, heap: Heap, threads, seeds, rounds: int):
+    """The jobs on a Heap, or on a structs.Pma (the same kernel compiled for
+    the bump heap); mode MODE_WARP (warp-collaborative calls, default) or
+    MODE_PLAIN (every thread calls malloc / free itself)."""
+
+    def __init__(self, heap, threads, seeds, rounds: int, mode: int | None = None):
         self.heap = heap
         jobs = _jobs(threads, seeds)
         b = c_void_p()
-        check(lib().kma_batch_create(heap.handle, jobs, len(jobs), rounds, byref(b)), "kma_batch_create")
+        if isinstance(heap, Heap):
+            check(lib().kma_batch_create(heap.handle, jobs, len(jobs), rounds, byref(b)), "kma_batch_create")
+        else:
+            check(lib().kma_batch_create_pma(heap.handle, jobs, len(jobs), rounds, byref(b)),
+                  "kma_batch_create_pma")
         self._b = b
         self.items = int(lib().kma_batch_items(b))
         self.rounds = rounds
+        if mode is not None:
+            check(lib().kma_batch_set_mode(b, mode), "kma_batch_set_mode")
 
     def close(self) -> None:
         b = getattr(self, "_b", None)

@@ -10,6 +10,12 @@
  * class in shared memory and hands them to the warp's next mallocs of that
  * class; cached blocks stay allocated in the heap, and the warp frees them
  * when the kernel ends.
+ *
+ * The kernel is a template on the heap (kma_backend.cuh: KMA, or the PMA
+ * bump heap, which frees nothing) and on the call style: the
+ * warp-collaborative calls, or the plain per-thread malloc / free of the
+ * reference on the same job set (the denominator the batched form is
+ * measured against).  The warp cache needs the KMA heap's size classes.
  */
 #include <string.h>
 #include <stdlib.h>
@@ -18,6 +24,8 @@
 
 #include "kma_internal.h"
 #include "kma_batch.h"
+#include "kma_structs.h"
+#include "kma_backend.cuh"
 #include "kma_wl_common.cuh"
 
 #define BT_CAP 16        /* live blocks a work-item keeps (lifetimes past this retire early) */
@@ -32,13 +40,16 @@ struct bt_dev {
 	const uint32_t *zipf;      /* [BT_ZIPF_N] cumulative thresholds of 2^32 */
 	uint64_t *rng;             /* [items] */
 	uint32_t *nlive;           /* [items] */
-	uint32_t *off4;            /* [BT_CAP * items] block offset from sb_base / 4 */
+	uint32_t *off4;            /* [BT_CAP * items] block offset from the heap base / unit (bt_unit) */
 	uint32_t *meta;            /* [BT_CAP * items] size/8 | expiry round << 16 */
 	unsigned long long *stats; /* kma_batch_stats order */
 };
 
 struct kma_batch_s {
-	kma_heap_s *heap;
+	kma_heap_s *heap;  /* KMA heap, or NULL */
+	kma_pma_s *pma;    /* PMA heap, or NULL */
+	int device;
+	int mode;          /* KMA_MODE_WARP (default) or KMA_MODE_PLAIN */
 	bt_dev d;
 	void *scratch;
 	uint64_t items;
@@ -85,66 +96,97 @@ struct bt_cache {
 	uint32_t *hint; /* the warp's kma_malloc_warp hint words */
 };
 
+/* Offsets in the live table are 32-bit multiples of the heap's block
+ * alignment: 4 bytes (KMA: 16 GiB heaps), 8 (PMA with the jobs' sizes,
+ * multiples of 8: 32 GiB). */
+template <class B> struct bt_unit;
+template <> struct bt_unit<kma_backend_kma> { static constexpr uint32_t shift = 2; };
+template <> struct bt_unit<kma_backend_pma> { static constexpr uint32_t shift = 3; };
+
+template <class B>
+__device__ __forceinline__ void *bt_block(typename B::heap *h, uint32_t off)
+{
+	return B::base(h) + ((size_t)off << bt_unit<B>::shift);
+}
+template <class B>
+__device__ __forceinline__ uint32_t bt_off(typename B::heap *h, const void *p)
+{
+	return (uint32_t)(((const unsigned char *)p - B::base(h)) >> bt_unit<B>::shift);
+}
+__device__ __forceinline__ uint32_t bt_bytes(uint32_t meta) { return (meta & 0x3ffu) * 8u; }
+
 /* Free q (NULL allowed) of n bytes: into the warp cache when it has room
  * for q's class, else to the heap.  Every lane of the warp calls it. */
-__device__ __forceinline__ void bt_free(kma_heap *h, const bt_cache &cc, uint32_t lane, void *q, uint32_t n,
+template <class B, bool WARP>
+__device__ __forceinline__ void bt_free(typename B::heap *h, const bt_cache &cc, uint32_t lane, void *q, uint32_t n,
 		bt_counters &ct)
 {
 	bool keep = false;
-	if (cc.depth && q) {
-		int c = kma_class_of(h, n);
-		if (c >= 0) {
-			int s = atomicAdd(&cc.cnt[c], 1);
-			if (s < (int)cc.depth) {
-				cc.slot[c * cc.depth + s] = (uint32_t)(((unsigned char *)q - h->sb_base) >> 2);
-				keep = true;
-				ct.puts++;
+	if constexpr (WARP && B::id == KMA_BACKEND_ID_KMA) {
+		if (cc.depth && q) {
+			int c = kma_class_of(h, n);
+			if (c >= 0) {
+				int s = atomicAdd(&cc.cnt[c], 1);
+				if (s < (int)cc.depth) {
+					cc.slot[c * cc.depth + s] = bt_off<B>(h, q);
+					keep = true;
+					ct.puts++;
+				}
 			}
 		}
+		if (cc.depth) {
+			__syncwarp();
+			if (lane < BT_NCLS && cc.cnt[lane] > (int)cc.depth)
+				cc.cnt[lane] = (int)cc.depth;
+			__syncwarp();
+		}
 	}
-	if (cc.depth) {
-		__syncwarp();
-		if (lane < BT_NCLS && cc.cnt[lane] > (int)cc.depth)
-			cc.cnt[lane] = (int)cc.depth;
-		__syncwarp();
-	}
-	kma_free_warp(h, keep ? NULL : q);
+	if (WARP)
+		B::free_block_warp(h, keep ? NULL : q);
+	else if (q)
+		B::free_block(h, q);
 }
 
 /* Malloc n bytes for lanes with `want`: from the warp cache when it holds
  * a block of n's class, else from the heap.  Every lane calls it. */
-__device__ __forceinline__ void *bt_malloc(kma_heap *h, const bt_cache &cc, uint32_t lane, bool want, uint32_t n,
-		bt_counters &ct)
+template <class B, bool WARP>
+__device__ __forceinline__ void *bt_malloc(typename B::heap *h, const bt_cache &cc, uint32_t lane, bool want,
+		uint32_t n, bt_counters &ct)
 {
 	void *p = NULL;
 	bool need = want;
-	if (cc.depth) {
-		if (want) {
-			int c = kma_class_of(h, n);
-			if (c >= 0) {
-				int old = atomicSub(&cc.cnt[c], 1);
-				if (old > 0) {
-					p = h->sb_base + ((size_t)cc.slot[c * cc.depth + old - 1] << 2);
-					need = false;
-					ct.hits++;
+	if constexpr (WARP && B::id == KMA_BACKEND_ID_KMA) {
+		if (cc.depth) {
+			if (want) {
+				int c = kma_class_of(h, n);
+				if (c >= 0) {
+					int old = atomicSub(&cc.cnt[c], 1);
+					if (old > 0) {
+						p = bt_block<B>(h, cc.slot[c * cc.depth + old - 1]);
+						need = false;
+						ct.hits++;
+					}
 				}
 			}
+			__syncwarp();
+			if (lane < BT_NCLS && cc.cnt[lane] < 0)
+				cc.cnt[lane] = 0;
+			__syncwarp();
 		}
-		__syncwarp();
-		if (lane < BT_NCLS && cc.cnt[lane] < 0)
-			cc.cnt[lane] = 0;
-		__syncwarp();
+		void *q = kma_malloc_warp(h, need ? (size_t)n : B::no_request, nullptr, cc.hint);
+		return need ? q : p;
+	} else if constexpr (WARP) {
+		void *q = B::alloc_warp(h, need ? (size_t)n : B::no_request);
+		return need ? q : p;
+	} else {
+		return need ? B::alloc(h, n) : p;
 	}
-	void *q = kma_malloc_warp(h, need ? (size_t)n : ~(size_t)0, nullptr, cc.hint);
-	return need ? q : p;
 }
 
-__device__ __forceinline__ void *bt_block(kma_heap *h, uint32_t off4) { return h->sb_base + ((size_t)off4 << 2); }
-__device__ __forceinline__ uint32_t bt_bytes(uint32_t meta) { return (meta & 0x3ffu) * 8u; }
-
 /* One round of every lane's item (act = the lane has one). */
-__device__ __forceinline__ void bt_round(kma_heap *h, const bt_dev &w, const bt_cache &cc, uint32_t lane, bool act,
-		uint64_t g, uint32_t r, uint64_t &rng, uint32_t &nl, bt_counters &ct)
+template <class B, bool WARP>
+__device__ __forceinline__ void bt_round(typename B::heap *h, const bt_dev &w, const bt_cache &cc, uint32_t lane,
+		bool act, uint64_t g, uint32_t r, uint64_t &rng, uint32_t &nl, bt_counters &ct)
 {
 	const uint32_t mask = 0xffffffffu;
 	const uint64_t items = w.items;
@@ -165,12 +207,12 @@ __device__ __forceinline__ void bt_round(kma_heap *h, const bt_dev &w, const bt_
 		uint32_t qn = 0;
 		if (mine) {
 			const uint64_t e = (uint64_t)i * items + o_g;
-			q = bt_block(h, w.off4[e]);
+			q = bt_block<B>(h, w.off4[e]);
 			qn = bt_bytes(w.meta[e]);
 		}
 		if (coop_verify_blockwise(mask, lane, q, qn, (uint32_t)o_g))
 			ct.bad++;
-		bt_free(h, cc, lane, q, qn, ct);
+		bt_free<B, WARP>(h, cc, lane, q, qn, ct);
 		if (q) {
 			ct.frees++;
 			ct.verify += qn;
@@ -199,12 +241,12 @@ __device__ __forceinline__ void bt_round(kma_heap *h, const bt_dev &w, const bt_
 		void *q = NULL;
 		uint32_t qn = 0;
 		if (full) {
-			q = bt_block(h, w.off4[g]);
+			q = bt_block<B>(h, w.off4[g]);
 			qn = bt_bytes(w.meta[g]);
 		}
 		if (coop_verify_blockwise(mask, lane, q, qn, tag))
 			ct.bad++;
-		bt_free(h, cc, lane, q, qn, ct);
+		bt_free<B, WARP>(h, cc, lane, q, qn, ct);
 		if (full) {
 			ct.frees++;
 			ct.retired++;
@@ -219,17 +261,17 @@ __device__ __forceinline__ void bt_round(kma_heap *h, const bt_dev &w, const bt_
 	/* 3. this round's block */
 	uint32_t n = zipf_size(w.zipf, splitmix(rng));
 	uint32_t life = geom_quarter(splitmix(rng));
-	void *p = bt_malloc(h, cc, lane, act, n, ct);
+	void *p = bt_malloc<B, WARP>(h, cc, lane, act, n, ct);
 	if (act) {
 		ct.mallocs++;
 		if (p) {
-			w.off4[(uint64_t)nl * items + g] = (uint32_t)(((unsigned char *)p - h->sb_base) >> 2);
+			w.off4[(uint64_t)nl * items + g] = bt_off<B>(h, p);
 			w.meta[(uint64_t)nl * items + g] = (n / 8u) | ((r + life) << 16);
 			nl++;
 			ct.fill += n;
 		} else {
 			ct.nulls++;
-			if (n > h->max_request)
+			if (n > B::max_request(h))
 				ct.refused++;
 		}
 	}
@@ -237,7 +279,8 @@ __device__ __forceinline__ void bt_round(kma_heap *h, const bt_dev &w, const bt_
 	coop_fill(mask, lane, act ? p : NULL, n, tag);
 }
 
-__global__ void __launch_bounds__(512, 2) k_bt_rounds(kma_heap *h, bt_dev w, uint32_t depth)
+template <class B, bool WARP>
+__global__ void __launch_bounds__(512, 2) k_bt_rounds(typename B::heap *h, bt_dev w, uint32_t depth)
 {
 	extern __shared__ int bt_smem[];
 	const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -260,7 +303,7 @@ __global__ void __launch_bounds__(512, 2) k_bt_rounds(kma_heap *h, bt_dev w, uin
 			bool act = g < w.items;
 			uint64_t rng = act ? w.rng[g] : 0;
 			uint32_t nl = act ? w.nlive[g] : 0;
-			bt_round(h, w, cc, lane, act, g, r, rng, nl, ct);
+			bt_round<B, WARP>(h, w, cc, lane, act, g, r, rng, nl, ct);
 			if (act) {
 				w.rng[g] = rng;
 				w.nlive[g] = nl;
@@ -276,9 +319,9 @@ __global__ void __launch_bounds__(512, 2) k_bt_rounds(kma_heap *h, bt_dev w, uin
 			if (k < total) {
 				uint32_t c = k / depth, s = k % depth;
 				if ((int)s < cc.cnt[c])
-					q = bt_block(h, cc.slot[c * depth + s]);
+					q = bt_block<B>(h, cc.slot[c * depth + s]);
 			}
-			kma_free_warp(h, q);
+			B::free_block_warp(h, q);
 		}
 	}
 	const uint32_t mask = 0xffffffffu;
@@ -320,11 +363,20 @@ __global__ void k_bt_begin(bt_dev w)
 	}
 }
 
-int bt_grid(uint32_t bd, uint32_t depth, int device, uint32_t *blocks, size_t *smem)
+/* the rounds kernel of b's heap and call style */
+const void *bt_kernel(const kma_batch_s *b)
+{
+	const bool warp = b->mode == KMA_MODE_WARP;
+	if (b->pma)
+		return warp ? (const void *)k_bt_rounds<kma_backend_pma, true> : (const void *)k_bt_rounds<kma_backend_pma, false>;
+	return warp ? (const void *)k_bt_rounds<kma_backend_kma, true> : (const void *)k_bt_rounds<kma_backend_kma, false>;
+}
+
+int bt_grid(const kma_batch_s *b, uint32_t bd, uint32_t depth, int device, uint32_t *blocks, size_t *smem)
 {
 	*smem = (size_t)(bd / 32) * (2 * BT_NCLS + BT_NCLS * depth) * 4;
 	int per_sm = 0, sms = 0;
-	KMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bt_rounds, (int)bd, *smem));
+	KMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bt_kernel(b), (int)bd, *smem));
 	KMA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
 	*blocks = (uint32_t)((per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1));
 	return KMA_OK;
@@ -332,20 +384,39 @@ int bt_grid(uint32_t bd, uint32_t depth, int device, uint32_t *blocks, size_t *s
 
 int bt_enqueue(kma_batch_t b, uint32_t bd, uint32_t depth, uint32_t blocks, size_t smem, cudaStream_t st)
 {
-	int rc = kma_reset(b->heap, st);
+	int rc = b->pma ? kma_pma_reset(b->pma, st) : kma_reset(b->heap, st);
 	if (rc != KMA_OK)
 		return rc;
 	k_bt_begin<<<148 * 4, 256, 0, st>>>(b->d);
 	KMA_CUDA(cudaGetLastError());
-	k_bt_rounds<<<blocks, bd, smem, st>>>(b->heap->dh, b->d, depth);
+	const bool warp = b->mode == KMA_MODE_WARP;
+	if (b->pma && warp)
+		k_bt_rounds<kma_backend_pma, true><<<blocks, bd, smem, st>>>(b->pma->dp, b->d, depth);
+	else if (b->pma)
+		k_bt_rounds<kma_backend_pma, false><<<blocks, bd, smem, st>>>(b->pma->dp, b->d, depth);
+	else if (warp)
+		k_bt_rounds<kma_backend_kma, true><<<blocks, bd, smem, st>>>(b->heap->dh, b->d, depth);
+	else
+		k_bt_rounds<kma_backend_kma, false><<<blocks, bd, smem, st>>>(b->heap->dh, b->d, depth);
 	KMA_CUDA(cudaGetLastError());
 	return KMA_OK;
 }
 
-bool bt_params_ok(uint32_t bd, uint32_t depth)
+bool bt_shape_ok(uint32_t bd, uint32_t depth)
 {
 	return (bd == 128 || bd == 256 || bd == 512) && depth <= KMA_BATCH_MAX_CACHE;
 }
+
+bool bt_params_ok(const kma_batch_s *b, uint32_t bd, uint32_t depth)
+{
+	/* the warp cache keeps blocks by KMA size class */
+	if (depth && (b->pma || b->mode != KMA_MODE_WARP))
+		return false;
+	return bt_shape_ok(bd, depth);
+}
+
+int batch_create(kma_heap_s *h, kma_pma_s *pma, const kma_batch_job *jobs, uint32_t njobs, uint32_t rounds,
+		kma_batch_t *out);
 
 } /* namespace */
 
@@ -355,10 +426,37 @@ extern "C" int kma_batch_create(kma_heap_t h, const kma_batch_job *jobs, uint32_
 	if (!out)
 		return KMA_EINVAL;
 	*out = NULL;
-	if (!h || !jobs || njobs == 0 || njobs > 4096 || rounds == 0 || rounds > 60000)
-		return KMA_EINVAL;
 	/* block offsets are kept as 32-bit multiples of 4 bytes */
-	if (h->hh.region_bytes > (1ull << 34))
+	if (!h || h->hh.region_bytes > (1ull << 34))
+		return KMA_EINVAL;
+	return batch_create(h, NULL, jobs, njobs, rounds, out);
+}
+
+extern "C" int kma_batch_create_pma(kma_pma_t p, const kma_batch_job *jobs, uint32_t njobs, uint32_t rounds,
+		kma_batch_t *out)
+{
+	if (!out)
+		return KMA_EINVAL;
+	*out = NULL;
+	/* 32-bit multiples of 8 bytes (the jobs' sizes keep bump blocks 8-aligned) */
+	if (!p || p->bytes > (1ull << 35))
+		return KMA_EINVAL;
+	return batch_create(NULL, p, jobs, njobs, rounds, out);
+}
+
+extern "C" int kma_batch_set_mode(kma_batch_t b, int mode)
+{
+	if (!b || (mode != KMA_MODE_WARP && mode != KMA_MODE_PLAIN))
+		return KMA_EINVAL;
+	b->mode = mode;
+	return KMA_OK;
+}
+
+namespace {
+int batch_create(kma_heap_s *h, kma_pma_s *pma, const kma_batch_job *jobs, uint32_t njobs, uint32_t rounds,
+		kma_batch_t *out)
+{
+	if (!jobs || njobs == 0 || njobs > 4096 || rounds == 0 || rounds > 60000)
 		return KMA_EINVAL;
 	std::vector<uint64_t> first(njobs + 1, 0), seed(njobs);
 	for (uint32_t j = 0; j < njobs; j++) {
@@ -380,11 +478,15 @@ extern "C" int kma_batch_create(kma_heap_t h, const kma_batch_job *jobs, uint32_
 			zipf[k - 1] = k == BT_ZIPF_N ? 0xffffffffu : (uint32_t)(t >= 4294967295.0 ? 4294967295.0 : t);
 		}
 	}
-	kma_device_guard g(h->device);
+	const int device = h ? h->device : pma->device;
+	kma_device_guard g(device);
 	kma_batch_s *b = (kma_batch_s *)calloc(1, sizeof(*b));
 	if (!b)
 		return KMA_ENOMEM;
 	b->heap = h;
+	b->pma = pma;
+	b->device = device;
+	b->mode = KMA_MODE_WARP;
 	b->items = items;
 	size_t o_first = 0, o_seed = o_first + (njobs + 1) * 8, o_zipf = o_seed + njobs * 8;
 	size_t o_rng = (o_zipf + BT_ZIPF_N * 4 + 255) & ~(size_t)255;
@@ -421,12 +523,13 @@ extern "C" int kma_batch_create(kma_heap_t h, const kma_batch_job *jobs, uint32_
 	*out = b;
 	return KMA_OK;
 }
+} /* namespace */
 
 extern "C" int kma_batch_destroy(kma_batch_t b)
 {
 	if (!b)
 		return KMA_EINVAL;
-	kma_device_guard g(b->heap->device);
+	kma_device_guard g(b->device);
 	if (b->exec)
 		cudaGraphExecDestroy(b->exec);
 	if (b->graph)
@@ -444,12 +547,12 @@ extern "C" int kma_batch_run(kma_batch_t b, uint32_t block_dim, uint32_t cache_d
 		return KMA_EINVAL;
 	if (block_dim == 0)
 		block_dim = 256;
-	if (!bt_params_ok(block_dim, cache_depth))
+	if (!bt_params_ok(b, block_dim, cache_depth))
 		return KMA_EINVAL;
-	kma_device_guard g(b->heap->device);
+	kma_device_guard g(b->device);
 	uint32_t blocks;
 	size_t smem;
-	int rc = bt_grid(block_dim, cache_depth, b->heap->device, &blocks, &smem);
+	int rc = bt_grid(b, block_dim, cache_depth, b->device, &blocks, &smem);
 	if (rc != KMA_OK)
 		return rc;
 	return bt_enqueue(b, block_dim, cache_depth, blocks, smem, kma_stream(stream));
@@ -461,12 +564,12 @@ extern "C" int kma_batch_capture(kma_batch_t b, uint32_t block_dim, uint32_t cac
 		return KMA_EINVAL;
 	if (block_dim == 0)
 		block_dim = 256;
-	if (!bt_params_ok(block_dim, cache_depth))
+	if (!bt_params_ok(b, block_dim, cache_depth))
 		return KMA_EINVAL;
-	kma_device_guard g(b->heap->device);
+	kma_device_guard g(b->device);
 	uint32_t blocks;
 	size_t smem;
-	int rc = bt_grid(block_dim, cache_depth, b->heap->device, &blocks, &smem);
+	int rc = bt_grid(b, block_dim, cache_depth, b->device, &blocks, &smem);
 	if (rc != KMA_OK)
 		return rc;
 	if (b->exec) {
@@ -501,7 +604,7 @@ extern "C" int kma_batch_launch(kma_batch_t b, void *stream)
 {
 	if (!b || !b->exec)
 		return KMA_EINVAL;
-	kma_device_guard g(b->heap->device);
+	kma_device_guard g(b->device);
 	KMA_CUDA(cudaGraphLaunch(b->exec, kma_stream(stream)));
 	return KMA_OK;
 }
@@ -510,7 +613,7 @@ extern "C" int kma_batch_stats_get(kma_batch_t b, void *stream, kma_batch_stats 
 {
 	if (!b || !out)
 		return KMA_EINVAL;
-	kma_device_guard g(b->heap->device);
+	kma_device_guard g(b->device);
 	unsigned long long v[16];
 	cudaStream_t st = kma_stream(stream);
 	KMA_CUDA(cudaMemcpyAsync(v, b->d.stats, sizeof(v), cudaMemcpyDeviceToHost, st));
@@ -542,7 +645,7 @@ extern "C" int kma_batch_autotune(const kma_batch_job *jobs, uint32_t njobs, uin
 			return KMA_EINVAL;
 	for (uint32_t i = 0; i < n_bd; i++)
 		for (uint32_t k = 0; k < n_depth; k++)
-			if (!bt_params_ok(block_dims[i], depths[k]))
+			if (!bt_shape_ok(block_dims[i], depths[k]))
 				return KMA_EINVAL;
 	kma_device_guard g(device);
 	if (!g.ok)

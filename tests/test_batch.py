@@ -90,3 +90,40 @@ def test_gpu_batch_autotune_reports_every_config():
     assert entries[best]["serves_all"] and entries[best]["refused"] == 0
     rate = [(e["mallocs"] - e["nulls"] + e["frees"]) / e["ms"] if e["serves_all"] else 0 for e in entries]
     assert rate[best] == max(rate)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sb_log2", [12, 14])
+def test_gpu_batch_plain_calls_invariants(sb_log2):
+    """The same jobs with every thread calling kma_malloc / kma_free itself
+    (the reference's per-work-item calls): tags intact, every block freed,
+    the heap canonically empty."""
+    from kma_b200 import MODE_PLAIN, Heap
+    from kma_b200.batch import Batch
+    seeds = list(range(201, 201 + len(SMALL_THREADS)))
+    with Heap((256 << 20) >> sb_log2, sb_log2) as h, \
+            Batch(h, SMALL_THREADS, seeds, rounds=10, mode=MODE_PLAIN) as b:
+        b.run(block_dim=256, cache_depth=0)
+        st = b.stats()
+        assert st["bad_tags"] == 0 and st["mallocs"] == sum(SMALL_THREADS) * 10
+        assert st["frees"] == st["mallocs"] - st["nulls"]
+        assert st["nulls"] == st["refused"]  # only the sizes 4 KiB superblocks cannot serve
+        _check_empty(h)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "warp"])
+def test_gpu_batch_on_pma(mode):
+    """The batch kernel compiled for the bump heap: every tag intact, and
+    the heap head is exactly the bytes handed out (frees do nothing)."""
+    from kma_b200.batch import Batch
+    from kma_b200.structs import Pma
+    seeds = list(range(301, 301 + len(SMALL_THREADS)))
+    with Pma(1 << 30) as p, Batch(p, SMALL_THREADS, seeds, rounds=10, mode=mode) as b:
+        b.run(block_dim=256, cache_depth=0)
+        st = b.stats()
+        assert st["bad_tags"] == 0 and st["nulls"] == 0 and st["refused"] == 0
+        assert st["mallocs"] == sum(SMALL_THREADS) * 10 and st["frees"] == st["mallocs"]
+        assert p.head() == st["fill_bytes"]
+        with pytest.raises(Exception):
+            b.run(block_dim=256, cache_depth=2)  # the warp cache needs KMA size classes
