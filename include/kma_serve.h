@@ -73,6 +73,13 @@ typedef struct kma_serve_summary {
 
 int kma_serve_create(kma_heap_t h, const kma_serve_cfg *cfg, kma_serve_t *out);
 int kma_serve_destroy(kma_serve_t s);
+/* Call style of later runs: KMA_MODE_WARP (the default: each warp's page
+ * mallocs and frees go to the heap as one warp-collaborative call) or
+ * KMA_MODE_PLAIN (every vertex's thread calls kma_malloc / kma_free
+ * itself, the reference's per-work-item calls, kma.cl:279-373).  There is
+ * no PMA form: a heap that frees nothing cannot stay resident under a
+ * stream of requests. */
+int kma_serve_set_mode(kma_serve_t s, int mode);
 /* Expected heap bytes of a request of n vertices (the admission estimate). */
 uint64_t kma_serve_estimate(kma_serve_t s, uint32_t n_vertices);
 /* Serve `n` requests (sorted by arrival_s).  realtime != 0 releases each

@@ -209,6 +209,7 @@ SIGNATURES = [
                                     c_void_p, c_void_p, c_void_p, c_void_p]),
     # include/kma_serve.h
     ("kma_serve_create", c_int, [c_void_p, POINTER(KmaServeCfg), POINTER(c_void_p)]),
+    ("kma_serve_set_mode", c_int, [c_void_p, c_int]),
     ("kma_serve_destroy", c_int, [c_void_p]),
     ("kma_serve_estimate", c_uint64, [c_void_p, c_uint32]),
     ("kma_serve_run", c_int, [c_void_p, POINTER(KmaServeReq), c_uint32, c_int, POINTER(KmaServeResult),

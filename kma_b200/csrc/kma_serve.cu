@@ -78,6 +78,11 @@ __device__ __forceinline__ void sv_flush(unsigned long long *acc, int k, unsigne
 		atomicAdd(&acc[k], v);
 }
 
+/* WARP: the pages of a warp's vertices come from one warp-collaborative
+ * heap call per step (kma_malloc_warp); otherwise every vertex's thread
+ * calls kma_malloc itself (the reference's per-work-item calls, the
+ * denominator the served form is measured against). */
+template <bool WARP>
 __global__ void k_sv_build(sv_params p)
 {
 	uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -96,7 +101,9 @@ __global__ void k_sv_build(sv_params p)
 			chunk = chunk < deg - written ? chunk : deg - written;
 		}
 		/* one warp-collaborative heap call for every lane's page */
-		void *blk = kma_malloc_warp(p.heap, chunk ? (size_t)chunk * 4 + KMA_AL_PAGE_HDR : ~(size_t)0);
+		const size_t req = (size_t)chunk * 4 + KMA_AL_PAGE_HDR;
+		void *blk = WARP ? kma_malloc_warp(p.heap, chunk ? req : ~(size_t)0)
+				 : (chunk ? kma_malloc(p.heap, req) : nullptr);
 		if (chunk) {
 			mallocs++;
 			void *objs = blk ? kma_detail::al_page_init(l, blk, chunk) : nullptr;
@@ -147,6 +154,7 @@ __global__ void k_sv_verify(sv_params p)
 	sv_flush(p.acc, 5, bad);
 }
 
+template <bool WARP>
 __global__ void k_sv_free(sv_params p)
 {
 	uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -159,7 +167,10 @@ __global__ void k_sv_free(sv_params p)
 			pg = kma_detail::clq_dequeue<kma_detail::clq_link_aligned>(&l->queue, &l->err, KMA_STRUCT_SPIN);
 			more = pg != 0;
 		}
-		kma_free_warp(p.heap, reinterpret_cast<void *>(pg));
+		if (WARP)
+			kma_free_warp(p.heap, reinterpret_cast<void *>(pg));
+		else if (pg)
+			kma_free(p.heap, reinterpret_cast<void *>(pg));
 		if (pg)
 			frees++;
 	}
@@ -181,6 +192,7 @@ struct sv_slot {
 struct kma_serve_s {
 	kma_heap_s *heap;
 	kma_serve_cfg cfg;
+	int mode; /* KMA_MODE_WARP (default) or KMA_MODE_PLAIN */
 	uint32_t *deg_cdf;
 	uint32_t *chunks;
 	uint32_t nchunks;
@@ -228,6 +240,7 @@ extern "C" int kma_serve_create(kma_heap_t h, const kma_serve_cfg *cfg, kma_serv
 	if (!s)
 		return KMA_ENOMEM;
 	s->heap = h;
+	s->mode = KMA_MODE_WARP;
 	s->cfg = *cfg;
 	s->cfg.block_dim = bd;
 	/* pages fill their size class: objects = (class bytes - header) / 4 */
@@ -303,6 +316,14 @@ extern "C" int kma_serve_destroy(kma_serve_t s)
 	for (uint32_t i = 0; i < s->cfg.slots; i++)
 		cudaStreamSynchronize(s->slot[i].st);
 	sv_teardown(s);
+	return KMA_OK;
+}
+
+extern "C" int kma_serve_set_mode(kma_serve_t s, int mode)
+{
+	if (!s || (mode != KMA_MODE_WARP && mode != KMA_MODE_PLAIN))
+		return KMA_EINVAL;
+	s->mode = mode;
 	return KMA_OK;
 }
 
@@ -422,11 +443,17 @@ extern "C" int kma_serve_run(kma_serve_t s, const kma_serve_req *reqs, uint32_t 
 				rc = KMA_ECUDA;
 				break;
 			}
-			k_sv_build<<<blocks, bd, 0, sl.st>>>(p);
+			if (s->mode == KMA_MODE_WARP)
+				k_sv_build<true><<<blocks, bd, 0, sl.st>>>(p);
+			else
+				k_sv_build<false><<<blocks, bd, 0, sl.st>>>(p);
 			if (ring)
 				cudaMemcpyAsync(&sl.host[7], &s->heap->dh->ring_avail.v, 4, cudaMemcpyDeviceToHost, sl.st);
 			k_sv_verify<<<blocks, bd, 0, sl.st>>>(p);
-			k_sv_free<<<blocks, bd, 0, sl.st>>>(p);
+			if (s->mode == KMA_MODE_WARP)
+				k_sv_free<true><<<blocks, bd, 0, sl.st>>>(p);
+			else
+				k_sv_free<false><<<blocks, bd, 0, sl.st>>>(p);
 			cudaMemcpyAsync(sl.host, sl.acc, 6 * 8, cudaMemcpyDeviceToHost, sl.st);
 			if (cudaGetLastError() != cudaSuccess || cudaEventRecord(sl.end, sl.st) != cudaSuccess) {
 				rc = KMA_ECUDA;

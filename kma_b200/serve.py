@@ -26,12 +26,16 @@ def c5_requests(seed: int, n: int, rate: float, nmin: int = 1000, nmax: int = 4_
 
 class Server:
     def __init__(self, heap: Heap, slots: int = 8, max_vertices: int = 4_000_000, deg_max: int = 4096,
-                 gamma: float = 2.1, occupancy_limit: float = 0.85, block_dim: int = 256):
+                 gamma: float = 2.1, occupancy_limit: float = 0.85, block_dim: int = 256, mode: int | None = None):
+        """mode: MODE_WARP (default, warp-collaborative page mallocs and
+        frees) or MODE_PLAIN (every vertex's thread calls malloc / free)."""
         self.heap = heap
         self.cfg = KmaServeCfg(slots, max_vertices, deg_max, block_dim, gamma, occupancy_limit)
         s = c_void_p()
         check(lib().kma_serve_create(heap.handle, byref(self.cfg), byref(s)), "kma_serve_create")
         self._s = s
+        if mode is not None:
+            check(lib().kma_serve_set_mode(s, mode), "kma_serve_set_mode")
 
     def close(self) -> None:
         s = getattr(self, "_s", None)

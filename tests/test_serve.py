@@ -104,3 +104,22 @@ def test_gpu_serve_admission_respects_occupancy():
         assert res[6]["status"] == ("too_big" if est_big > limit else "ok")
         assert summ["max_running"] * s.estimate(n_ok) <= limit
         _empty(h)
+
+
+@pytest.mark.gpu
+def test_gpu_serve_plain_calls_equal_warp_calls():
+    """The same requests with every vertex's thread calling kma_malloc /
+    kma_free itself give the same results as the warp-collaborative calls
+    (results do not depend on where the blocks landed), and empty the heap."""
+    from kma_b200 import MODE_PLAIN, Heap
+    from kma_b200.serve import Server
+    nv, seeds, _ = c5_requests(13, 8, rate=0, nmin=1000, nmax=80_000)
+    with Heap(65536, 14) as h:
+        with Server(h, slots=4, max_vertices=100_000) as s:
+            warp, _ = s.run(nv, seeds)
+        with Server(h, slots=4, max_vertices=100_000, mode=MODE_PLAIN) as s:
+            plain, _ = s.run(nv, seeds)
+        for a, b in zip(warp, plain):
+            assert a["status"] == b["status"] == "ok"
+            assert (a["checksum"], a["edges"], a["mallocs"]) == (b["checksum"], b["edges"], b["mallocs"])
+        _empty(h)
