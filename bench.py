@@ -225,26 +225,56 @@ def tree_expected(kinds, keys):
     return res, n_live
 
 
+def c3_line(kind: int, threads: int, per: int, shards: int) -> dict:
+    """One config-3 queue run: enqueue / dequeue rates and conservation."""
+    from kma_b200 import structs
+    st = structs.c3_queue(kind, threads, per, shards, seed=0xC3)
+    n = threads * per
+    ok = (st["out_count"] == n and st["out_xor"] == st["in_xor"] and st["out_sum"] == st["in_sum"]
+          and st["walk_ok"] == 1 and st["err"] == 0)
+    t = (st["enqueue_ms"] + st["dequeue_ms"]) / 1e3
+    return {"payloads": n, "threads": threads, "shards": shards, "warp_calls": bool(kind & structs.C3_WARP),
+            "conserved": bool(ok), "enqueue_mops": round(n / st["enqueue_ms"] / 1e3, 2),
+            "dequeue_mops": round(n / st["dequeue_ms"] / 1e3, 2), "mops": round(2 * n / t / 1e6, 2)}
+
+
+def time_batch(b, block_dim: int, depth: int, reps: int = 2) -> tuple[float, dict]:
+    """Mean device ms of a captured batch run (CUDA events on the capture
+    stream, one warm-up launch) and the counters of the last run."""
+    import torch
+    stream = torch.cuda.Stream()
+    b.capture(block_dim, depth, stream)
+    b.launch(stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        b.launch(stream)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps, b.stats(stream)
+
+
 def measure_forms(quick: bool = False) -> dict:
     """Config 3 (structures), 4 (batched, autotuned) and 5 (served) on this
-    GPU: each its own workload at its configured size, timed on the device."""
+    GPU: each its own workload at its configured size, timed on the device,
+    beside the plain per-thread calls on the same work and the PMA heap."""
     import numpy as np
-    from kma_b200 import Heap, structs
-    from kma_b200.batch import autotune, c4_jobs
+    from kma_b200 import MODE_PLAIN, Heap, structs
+    from kma_b200.batch import Batch, autotune, c4_jobs
     from kma_b200.serve import Server, c5_requests
     out = {}
-    # config 3: 2^24 payloads by 2^18 threads x 64; tree 2^22 ops 50/30/20
+    # config 3: one clQueue and one clIndexedQueue (the reference's single
+    # structures), 2^24 payloads by 2^18 threads x 64, through the warp
+    # forms; the per-thread calls on one queue at 2^16 payloads (at full
+    # size their waits on the one head run out); 4096 independent shards
+    # as an extra
     c3 = {}
+    big = (1 << 18, 64) if not quick else (1 << 14, 64)
     for name, kind in (("clqueue", structs.C3_CLQUEUE), ("iqueue", structs.C3_IQUEUE)):
-        for shards, thr, per in ((4096, 1 << 18, 64), (1, 1 << 12, 16)):
-            st = structs.c3_queue(kind, thr, per, shards, seed=0xC3)
-            n = thr * per
-            ok = (st["out_count"] == n and st["out_xor"] == st["in_xor"] and st["out_sum"] == st["in_sum"]
-                  and st["walk_ok"] == 1 and st["err"] == 0)
-            c3[f"{name}_shards{shards}"] = {
-                "payloads": n, "threads": thr, "conserved": bool(ok),
-                "enqueue_mops": round(n / st["enqueue_ms"] / 1e3, 1),
-                "dequeue_mops": round(n / st["dequeue_ms"] / 1e3, 1)}
+        c3[f"{name}_single"] = c3_line(kind | structs.C3_WARP, big[0], big[1], 1)
+        c3[f"{name}_single_per_thread_small"] = c3_line(kind, 1 << 12, 16, 1)
+        c3[f"{name}_shards4096"] = c3_line(kind, big[0], big[1], 4096)
+        c3[f"{name}_shards4096_warp"] = c3_line(kind | structs.C3_WARP, big[0], big[1], 4096)
     rng = np.random.default_rng(0xC3)
     nt = 1 << 22
     kinds = rng.choice(3, size=nt, p=(0.5, 0.3, 0.2)).astype(np.uint8)
@@ -255,40 +285,79 @@ def measure_forms(quick: bool = False) -> dict:
                   "equals_sequential": bool(np.array_equal(res, exp) and st["live_keys"] == n_live
                                             and st["sorted"] == 1 and st["err"] == 0)}
     out["structures_c3"] = c3
-    # config 4: 64 jobs of 1k..1M threads, 16 GiB heap, autotuned
+    # config 4: 64 jobs of 1k..1M threads, 16 GiB heap, autotuned over the
+    # geometries that serve every size the jobs draw; then the same jobs
+    # with plain per-thread calls, and on a PMA heap
     t, sd = c4_jobs()
     grid = dict(sb_log2s=(12, 14, 16), block_dims=(128, 256, 512), depths=(0, 2, 4)) if not quick else \
-        dict(sb_log2s=(12,), block_dims=(256,), depths=(0, 4))
+        dict(sb_log2s=(12, 14), block_dims=(256,), depths=(0, 4))
     entries, best = autotune(t, sd, rounds=16, heap_bytes=16 << 30, warmup=1, reps=2, **grid)
     b = entries[best]
-    out["batched_c4"] = {
-        "jobs": 64, "work_items": int(t.sum()), "rounds": 16, "heap_bytes": 16 << 30,
-        "best": {"sb_size": b["sb_size"], "block_dim": b["block_dim"], "cache_depth": b["cache_depth"],
-                 "mops": b["mops"], "ms_per_launch": b["ms"],
-                 "null_frac": round(b["nulls"] / b["mallocs"], 4), "bad_tags": b["bad_tags"]},
-        "grid": [[e["sb_size"], e["block_dim"], e["cache_depth"], e["mops"],
-                  round(e["nulls"] / e["mallocs"], 4)] for e in entries],
-        "grid_cols": ["sb_size", "block_dim", "cache_depth", "mops", "null_frac"],
-        "launch": "one CUDA graph per configuration: heap reset + job seeding + one persistent kernel"}
-    # config 5: 64 GiB resident heap, Poisson arrivals at swept rates
+
+    def nulls(e):
+        return {"null_frac": round(e["nulls"] / e["mallocs"], 4), "refused": e["refused"],
+                "exhausted": e["nulls"] - e["refused"]}
+    c4 = {"jobs": 64, "work_items": int(t.sum()), "rounds": 16, "heap_bytes": 16 << 30,
+          "best": {"sb_size": b["sb_size"], "block_dim": b["block_dim"], "cache_depth": b["cache_depth"],
+                   "mops": b["mops"], "ms_per_launch": b["ms"], **nulls(b), "bad_tags": b["bad_tags"]},
+          "grid": [[e["sb_size"], e["block_dim"], e["cache_depth"], e["mops"], e["serves_all"],
+                    round(e["nulls"] / e["mallocs"], 4), e["refused"]] for e in entries],
+          "grid_cols": ["sb_size", "block_dim", "cache_depth", "mops", "serves_all", "null_frac", "refused"],
+          "launch": "one CUDA graph per configuration: heap reset + job seeding + one persistent kernel"}
+    lg = b["sb_size"].bit_length() - 1
+    with Heap((16 << 30) >> lg, lg) as h, Batch(h, t, sd, rounds=16, mode=MODE_PLAIN) as pb:
+        ms, stp = time_batch(pb, b["block_dim"], 0)
+    plain_mops = (stp["mallocs"] + stp["frees"]) / ms / 1e3
+    c4["plain_same_workload"] = {"sb_size": b["sb_size"], "block_dim": b["block_dim"], "mops": round(plain_mops, 1),
+                                 "ms_per_launch": round(ms, 3), **nulls(stp), "bad_tags": stp["bad_tags"],
+                                 "calls": "kma_malloc / kma_free per thread"}
+    c4["batched_over_plain_same_workload"] = round(b["mops"] / plain_mops, 3)
+    pma = {}
+    with structs.Pma(32 << 30) as p:
+        for mname, mode in (("warp", 1), ("plain", MODE_PLAIN)):
+            with Batch(p, t, sd, rounds=16, mode=mode) as pb:
+                ms, stp = time_batch(pb, b["block_dim"], 0)
+            pma[mname] = {"mops": round((stp["mallocs"] + stp["frees"]) / ms / 1e3, 1),
+                          "ms_per_launch": round(ms, 3), **nulls(stp), "bad_tags": stp["bad_tags"]}
+    c4["pma_32GiB"] = pma
+    out["batched_c4"] = c4
+    # config 5: 64 GiB resident heap, Poisson arrivals at swept rates, warp
+    # calls; the all-at-once load again with plain per-thread calls; and a
+    # 1 GiB heap with 64 slots, where the 85% occupancy admission, not the
+    # slots, bounds how many requests run at once
     served = []
-    with Heap((64 << 30) >> 14, 14) as h, Server(h, slots=16) as srv:
-        for rate in ((200, 3200, 0) if not quick else (3200,)):
-            nv, seeds, arr = c5_requests(0xC5, 300, rate=rate if rate else 1.0)
-            res_s, summ = srv.run(nv, seeds, arr if rate else None, realtime=bool(rate))
-            lat = np.array([r["latency_s"] for r in res_s if r["status"] == "ok"])
-            served.append({"rate_per_s": rate or "all at once", "requests": len(res_s),
-                           "ok": int(sum(r["status"] == "ok" for r in res_s)),
-                           "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
-                           "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
-                           "mops": round(summ["ops"] / summ["wall_s"] / 1e6, 1),
-                           "requests_per_s": round(len(res_s) / summ["wall_s"], 1),
-                           "max_running": summ["max_running"],
-                           "max_occupancy": round(summ["max_occupancy"], 4)})
+
+    def load(srv, rate, nreq=300, seed=0xC5, heap_bytes=64 << 30, calls="warp"):
+        nv, seeds, arr = c5_requests(seed, nreq, rate=rate if rate else 1.0)
+        res_s, summ = srv.run(nv, seeds, arr if rate else None, realtime=bool(rate))
+        ok = [r for r in res_s if r["status"] == "ok"]
+        lat = np.array([r["latency_s"] for r in ok]) if ok else np.zeros(1)
+        return {"rate_per_s": rate or "all at once", "heap_bytes": heap_bytes, "calls": calls,
+                "requests": len(res_s), "ok": len(ok),
+                "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 3),
+                "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 3),
+                "mops": round(summ["ops"] / summ["wall_s"] / 1e6, 1),
+                "requests_per_s": round(len(res_s) / summ["wall_s"], 1),
+                "max_running": summ["max_running"], "max_occupancy": round(summ["max_occupancy"], 4),
+                "max_reserved": round(summ["max_reserved"], 4), "admit_waits_for_room": summ["admit_waits"]}
+    with Heap((64 << 30) >> 14, 14) as h:
+        with Server(h, slots=16) as srv:
+            for rate in ((200, 3200, 0) if not quick else (3200, 0)):
+                served.append(load(srv, rate))
+        with Server(h, slots=16, mode=MODE_PLAIN) as srv:
+            served.append(load(srv, 0, calls="plain"))
         flags = h.error_flags()
+    with Heap((1 << 30) >> 14, 14) as h, Server(h, slots=64, max_vertices=4_000_000) as srv:
+        served.append(load(srv, 0, nreq=200, seed=0xC55, heap_bytes=1 << 30))
+        flags |= h.error_flags()
+    warp_all = next(x for x in served if x["rate_per_s"] == "all at once" and x["calls"] == "warp"
+                    and x["heap_bytes"] == 64 << 30)
+    plain_all = next(x for x in served if x["calls"] == "plain")
     out["served_c5"] = {"heap_bytes": 64 << 30, "slots": 16, "occupancy_limit": 0.85,
                         "graph": "N log-uniform 1k..4M vertices, degrees ~ d^-2.1 on 1..4096",
-                        "heap_error_flags": flags, "loads": served}
+                        "heap_error_flags": flags, "loads": served,
+                        "served_over_plain_same_workload": round(warp_all["mops"] / plain_all["mops"], 3)
+                        if plain_all["mops"] else None}
     out["graph_build"] = measure_graph_build(quick)
     return out
 
@@ -310,11 +379,11 @@ def measure_graph_build(quick: bool = False) -> dict:
     build is followed by the teardown that frees every block, and must give
     the edge multiset back and leave the heap canonically empty.  Two rank
     distributions: Zipf(1.1), where the hottest vertex's one link queue
-    takes a large share of all enqueues (it bounds the build: enqueues on
-    one queue serialise), and uniform."""
+    takes a large share of all enqueues, and uniform.  The same kernels
+    also run on a PMA heap (which frees nothing; reset between builds)."""
     import statistics
     import numpy as np
-    from kma_b200 import Heap, graph
+    from kma_b200 import Heap, graph, structs
     from kma_b200 import inspect as ins
     n_e, n_v = (1 << 22, 1 << 20) if not quick else (1 << 18, 1 << 16)
     threads = 148 * 1024
@@ -337,10 +406,21 @@ def measure_graph_build(quick: bool = False) -> dict:
             empty = ins.check_canonical_empty(h.snapshot(), h.bitmaps()) == []
             flags = h.error_flags()
         t = statistics.median(ms)
+        pms, pok = [], True
+        with structs.Pma(1 << 30) as p:
+            for _ in range(3):
+                p.reset()
+                st, _ = graph.build(p, e, threads=threads)
+                pms.append(float(st["build_ms"]))
+                pok = pok and all(int(st[k]) == v for k, v in want.items()) and \
+                    st["err"] == 0 and st["nulls"] == 0 and st["sorted"] == 1
+        tp = statistics.median(pms)
         out[name] = {"nodes": want["nodes"], "max_out_degree": max_out, "build_ms": round(t, 3),
                      "medges_per_s": round(n_e / t / 1e3, 2), "lost_adds": lost,
                      "edges_conserved": bool(ok), "empty_after_teardown": bool(empty),
-                     "heap_error_flags": flags}
+                     "heap_error_flags": flags,
+                     "pma": {"build_ms": round(tp, 3), "medges_per_s": round(n_e / tp / 1e3, 2),
+                             "edges_conserved": bool(pok)}}
     return out
 
 

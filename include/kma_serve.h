@@ -69,6 +69,11 @@ typedef struct kma_serve_summary {
 	uint32_t max_running;    /* most requests on the device at once */
 	uint32_t max_sb_in_use;  /* most superblocks in use seen after a build */
 	double max_occupancy;    /* max_sb_in_use / superblocks on the free list at reset */
+	double max_reserved;     /* most admission estimates held at once / heap bytes
+				  * (the admission rule keeps it <= occupancy_limit) */
+	uint32_t admit_waits;    /* admissions deferred because the heap room, not a
+				  * slot, was missing */
+	uint32_t pad;
 } kma_serve_summary;
 
 int kma_serve_create(kma_heap_t h, const kma_serve_cfg *cfg, kma_serve_t *out);

@@ -106,7 +106,8 @@ class KmaServeResult(Structure):
 
 class KmaServeSummary(Structure):
     _fields_ = [("wall_s", c_double), ("ops", c_uint64), ("max_running", c_uint32),
-                ("max_sb_in_use", c_uint32), ("max_occupancy", c_double)]
+                ("max_sb_in_use", c_uint32), ("max_occupancy", c_double), ("max_reserved", c_double),
+                ("admit_waits", c_uint32), ("pad", c_uint32)]
 
 
 class KmaGraphStats(Structure):

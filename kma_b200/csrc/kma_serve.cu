@@ -361,7 +361,8 @@ extern "C" int kma_serve_run(kma_serve_t s, const kma_serve_req *reqs, uint32_t 
 	};
 	std::deque<uint32_t> waiting;
 	uint32_t next = 0, done = 0, running = 0;
-	uint64_t reserved = 0;
+	uint64_t reserved = 0, max_reserved = 0;
+	bool room_wait = false;
 	int rc = KMA_OK;
 	double last_done = 0;
 	while (done < n && rc == KMA_OK) {
@@ -417,14 +418,21 @@ extern "C" int kma_serve_run(kma_serve_t s, const kma_serve_req *reqs, uint32_t 
 				progress = true;
 				continue;
 			}
-			if (reserved + est > limit)
-				break;
 			int free_slot = -1;
 			for (uint32_t i = 0; i < s->cfg.slots; i++)
 				if (s->slot[i].req < 0) {
 					free_slot = (int)i;
 					break;
 				}
+			if (reserved + est > limit) {
+				/* counted once per wait: a slot was free, the room was not */
+				if (free_slot >= 0 && !room_wait) {
+					sum->admit_waits++;
+					room_wait = true;
+				}
+				break;
+			}
+			room_wait = false;
 			if (free_slot < 0)
 				break;
 			sv_slot &sl = s->slot[free_slot];
@@ -463,6 +471,8 @@ extern "C" int kma_serve_run(kma_serve_t s, const kma_serve_req *reqs, uint32_t 
 			sl.req = (int)ri;
 			sl.reserved = est;
 			reserved += est;
+			if (reserved > max_reserved)
+				max_reserved = reserved;
 			res[ri].admit_s = now_s();
 			res[ri].slot = (uint32_t)free_slot;
 			res[ri].reserved_bytes = est;
@@ -488,5 +498,6 @@ extern "C" int kma_serve_run(kma_serve_t s, const kma_serve_req *reqs, uint32_t 
 	double first = n ? (realtime ? reqs[0].arrival_s : 0.0) : 0.0;
 	sum->wall_s = last_done > first ? last_done - first : 0.0;
 	sum->max_occupancy = pages ? (double)sum->max_sb_in_use / (double)pages : 0.0;
+	sum->max_reserved = heap_bytes ? (double)max_reserved / (double)heap_bytes : 0.0;
 	return rc;
 }

@@ -103,6 +103,10 @@ def test_gpu_serve_admission_respects_occupancy():
             assert r["reserved_bytes"] == s.estimate(n_ok)
         assert res[6]["status"] == ("too_big" if est_big > limit else "ok")
         assert summ["max_running"] * s.estimate(n_ok) <= limit
+        # the heap room, not the 8 slots, held requests back
+        assert summ["max_running"] < 8 and summ["admit_waits"] > 0
+        assert summ["max_reserved"] <= 0.85 + 1e-9
+        assert summ["max_reserved"] == pytest.approx(summ["max_running"] * s.estimate(n_ok) / (4096 * 16384))
         _empty(h)
 
 
