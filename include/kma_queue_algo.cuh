@@ -25,6 +25,22 @@
  * exactly as the reference's queues: same results, same head, tail and
  * links.
  *
+ * Chain log (optional).  A dequeue that takes k items must learn their
+ * addresses, and a linked list gives them one dependent load at a time.
+ * With a chain log, an append of a chain of k items (a warp's) also writes
+ * the k items into a log record and marks the chain's first link with the
+ * record's number and k.  A dequeue that finds a marked link at the head
+ * reads the record and checks every link it names with loads that do not
+ * depend on one another (one round trip, not k), and takes the whole
+ * chain with one move of the head.  A record is only a hint: records are
+ * reused round robin, so a dequeue takes a chain from its record only
+ * when the queue's current links say exactly what the record says, and
+ * walks otherwise.
+ *
+ * Log policy `LG` (a null pointer: no log) provides the items of record
+ * `recno` (records are reused modulo the log's size):
+ *   iq_item(recno, j)    index of item j        clq_item(recno, j)   pointer of item j
+ *
  * Policy `O` provides, on 64-bit words:
  *   ld(p)        acquire load        st(p, v)     release store
  *   ld_rlx(p)    relaxed load        st_rlx(p, v) relaxed store
@@ -61,8 +77,73 @@ const u64 POISON = 1ull;
 const int PTR_BITS = 48;
 const u64 PTR_MASK = (1ull << PTR_BITS) - 1ull;
 
+/* chain log records: numbers of 25 bits, chains of at most 32 items */
+const uint32_t LOG_RECNO_MASK = 0x1FFFFFFu;
+const uint32_t LOG_CHAIN_MAX = 32;
+
 KQ_FN u64 qp_ptr(u64 w) { return w & PTR_MASK; }
 KQ_FN u64 qp_next(u64 w, u64 ptr) { return (((w >> PTR_BITS) + 1ull) << PTR_BITS) | ptr; }
+
+/* A logged chain (at least 3 items) marks the top 16 bits of its first
+ * two links: first = CLQ_LOG | (length - 1) << 10 | record number bits
+ * 15..24, second = record number bits 0..14 (its top bit stays clear, so
+ * it never reads as a first mark).  Every other link has them clear;
+ * readers take the pointer with qp_ptr. */
+const u64 CLQ_LOG = 0x8000ull << PTR_BITS;
+KQ_FN u64 clq_mark_first(uint32_t recno, uint32_t len)
+{
+	return CLQ_LOG | ((u64)(((len - 1u) << 10) | ((recno >> 15) & 0x3FFu)) << PTR_BITS);
+}
+KQ_FN u64 clq_mark_second(uint32_t recno) { return (u64)(recno & 0x7FFFu) << PTR_BITS; }
+
+/* Up to k items [hp, ...] of the logged chain that starts at hp (its link
+ * v), if its record matches the links: fills out[], sets *nh to the item
+ * after them, returns how many (0: no usable record).  Reads only. */
+template <class O, class L, class LG>
+KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32_t k, u64 *nh)
+{
+	if (!log || !(v & CLQ_LOG) || k == 0)
+		return 0;
+	const uint32_t mark = (uint32_t)(v >> PTR_BITS);
+	const uint32_t len = ((mark >> 10) & 31u) + 1u;
+	const u64 second = qp_ptr(v);
+	if (len < 3 || second <= POISON)
+		return 0;
+	const u64 l1 = O::ld(L::at(second));
+	const uint32_t recno = ((mark & 0x3FFu) << 15) | ((uint32_t)(l1 >> PTR_BITS) & 0x7FFFu);
+	uint32_t m = len < k ? len : k;
+	for (uint32_t j = 0; j < m; j++)
+		out[j] = log->clq_item(recno, j);
+	const u64 after = m < len ? log->clq_item(recno, m) : 0ull;
+	if (out[0] != hp || (m > 1 && out[1] != second) || (m > 2 && out[2] != qp_ptr(l1)))
+		return 0;
+	/* record entries are 0 or item pointers (0 in a slot a chain has not
+	 * filled, or is refilling): none may be followed before it is known
+	 * to be an item */
+	for (uint32_t j = 3; j < m; j++)
+		if (out[j] <= POISON)
+			return 0;
+	u64 nx[LOG_CHAIN_MAX];
+	for (uint32_t j = 2; j < m; j++) /* independent loads */
+		nx[j] = O::ld(L::at(out[j]));
+	for (uint32_t j = 2; j + 1 < m; j++)
+		if (nx[j] == POISON || qp_ptr(nx[j]) != out[j + 1])
+			return 0;
+	u64 next = m == 1 ? second : (m == 2 ? qp_ptr(l1) : nx[m - 1]);
+	if (next == POISON)
+		return 0;
+	next = qp_ptr(next);
+	if (m < len) {
+		if (next != after)
+			return 0;
+	} else if (next == 0) {
+		/* the chain's last item has no successor yet: it stays, as the head */
+		next = out[m - 1];
+		m--;
+	}
+	*nh = next;
+	return m;
+}
 
 /* Append the chain first..last (its links already set, last's link 0,
  * all of it written before the call).  1, or 0 when a wait expired. */
@@ -104,8 +185,9 @@ KQ_FN int clq_append(u64 *headw, u64 *tailw, u64 first, u64 last, uint32_t limit
  * head, so the items behind it are read without further atomics and the
  * head moves past all of them with one store.  Taken items keep POISON
  * in their links. */
-template <class O, class L>
-KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint32_t limit, bool *timed_out)
+template <class O, class L, class LG>
+KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint32_t limit, bool *timed_out,
+		const LG *log)
 {
 	*timed_out = false;
 	uint32_t it = 0;
@@ -117,10 +199,15 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 		u64 *hl = L::at(hp);
 		/* look before taking: while another dequeuer holds the head item,
 		 * waiters only read its link */
-		if (O::ld_rlx(hl) == POISON) {
+		const u64 seen = O::ld(hl);
+		if (seen == POISON) {
 			O::pause(it++);
 			continue;
 		}
+		/* a logged chain at the head: check its record before the hold, so
+		 * the hold lasts only the exchange and the head check */
+		u64 nh = 0;
+		const uint32_t m = clq_chain_from_log<O, L>(log, hp, seen, out, k, &nh);
 		const u64 nx = O::xchg(hl, POISON);
 		if (nx == POISON) {
 			/* another dequeuer holds it, or it left the queue already */
@@ -134,17 +221,24 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 			O::pause(it++);
 			continue;
 		}
+		if (m && nx == seen) {
+			/* nothing moved since the check: the chain's links are those */
+			for (uint32_t j = 1; j < m; j++)
+				O::st_rlx(L::at(out[j]), POISON);
+			O::st(headw, qp_next(h, nh));
+			return m;
+		}
 		if (nx != 0) {
 			out[0] = hp;
 			uint32_t r = 1;
-			u64 cur = nx;
+			u64 cur = qp_ptr(nx);
 			while (r < k) {
 				const u64 n2 = O::ld(L::at(cur));
 				if (n2 == 0 || n2 == POISON)
 					break; /* cur is the last linked item: it stays, as the head */
 				O::st_rlx(L::at(cur), POISON);
 				out[r++] = cur;
-				cur = n2;
+				cur = qp_ptr(n2);
 			}
 			O::st(headw, qp_next(h, cur));
 			return r;
@@ -182,23 +276,72 @@ KQ_FN uint32_t tw_idx(u64 w) { return (uint32_t)w; }
 KQ_FN uint32_t tw_tag(u64 w) { return (uint32_t)(w >> 32); }
 KQ_FN u64 tw_make(uint32_t tag, uint32_t idx) { return ((u64)tag << 32) | idx; }
 
+/* Links need no ABA tag (nothing CASes them): a link's tag is 0, or, on
+ * the first link of a logged chain, IQ_LOG | record number (25 bits) << 5 |
+ * (chain length - 1).  Head keeps a counting tag. */
+const uint32_t IQ_LOG = 0x80000000u;
+KQ_FN uint32_t iq_log_tag(uint32_t recno, uint32_t len)
+{
+	return IQ_LOG | ((recno & LOG_RECNO_MASK) << 5) | (len - 1u);
+}
+
 /* Q provides u64 *link(uint32_t idx); every index the queue can hold,
  * and 0 (a zero word), has one. */
 template <class O, class Q>
 KQ_FN void iq_append(const Q &q, u64 *tailw, uint32_t first, uint32_t last)
 {
 	const u64 prev = O::xchg(tailw, tw_make(0, last));
-	u64 *pl = q.link(tw_idx(prev));
-	O::st(pl, tw_make(tw_tag(O::ld_rlx(pl)) + 1u, first));
+	O::st(q.link(tw_idx(prev)), tw_make(0, first));
 }
 
-/* Set item idx's link (to 0, or to the next item of a chain) before idx
- * is appended. */
+/* Set item idx's link (to 0, or to the next item of a chain; tag: 0, or
+ * iq_log_tag on a logged chain's first item) before idx is appended. */
 template <class O, class Q>
-KQ_FN void iq_set_link(const Q &q, uint32_t idx, uint32_t next)
+KQ_FN void iq_set_link(const Q &q, uint32_t idx, uint32_t next, uint32_t tag = 0)
 {
-	u64 *l = q.link(idx);
-	O::st_rlx(l, tw_make(tw_tag(O::ld_rlx(l)) + 1u, next));
+	O::st_rlx(q.link(idx), tw_make(tag, next));
+}
+
+/* Take up to k items [h0 = head, ...] of the logged chain that starts at
+ * the head, if its record matches the links: fills out[], sets *nh to the
+ * head after them, returns how many (0: no usable record).  l0 = h0's
+ * link.  The head is not moved here. */
+template <class O, class Q, class LG>
+KQ_FN uint32_t iq_chain_from_log(const Q &q, const LG *log, uint32_t h0, u64 l0, uint32_t *out, uint32_t k,
+		uint32_t *nh)
+{
+	const uint32_t tag = tw_tag(l0);
+	if (!log || !(tag & IQ_LOG) || k == 0)
+		return 0;
+	const uint32_t len = (tag & 31u) + 1u;
+	const uint32_t recno = (tag >> 5) & LOG_RECNO_MASK;
+	/* the record's items, and the link after each: item j -> item j+1 must
+	 * hold for the items taken and for the one that becomes the head */
+	uint32_t m = len < k ? len : k;
+	for (uint32_t j = 0; j < m; j++)
+		out[j] = log->iq_item(recno, j);
+	const uint32_t after = m < len ? log->iq_item(recno, m) : 0u;
+	if (out[0] != h0 || (len > 1 && m > 1 && out[1] != tw_idx(l0)) || (m == 1 && len > 1 && after != tw_idx(l0)))
+		return 0;
+	uint32_t nx[LOG_CHAIN_MAX];
+	for (uint32_t j = 1; j < m; j++) /* independent loads */
+		nx[j] = tw_idx(O::ld(q.link(out[j])));
+	for (uint32_t j = 1; j + 1 < m; j++)
+		if (nx[j] != out[j + 1])
+			return 0;
+	uint32_t next = m == 1 ? tw_idx(l0) : nx[m - 1];
+	if (m < len) {
+		if (next != after)
+			return 0;
+	} else if (next == 0) {
+		/* the chain's last item has no successor yet: it stays, as the head */
+		if (m == 1)
+			return 0;
+		next = out[m - 1];
+		m--;
+	}
+	*nh = next;
+	return m;
 }
 
 /* Dequeue up to k old dummies into out[] (indices, FIFO order).  Returns
@@ -207,13 +350,25 @@ KQ_FN void iq_set_link(const Q &q, uint32_t idx, uint32_t next)
  * chain behind the head first and moves the head past it with one CAS; a
  * head that moved meanwhile fails the CAS (its tag changed) and the walk
  * is retried. */
-template <class O, class Q>
-KQ_FN uint32_t iq_dequeue_n(const Q &q, u64 *headw, uint32_t *out, uint32_t k, uint32_t limit, bool *timed_out)
+template <class O, class Q, class LG>
+KQ_FN uint32_t iq_dequeue_n(const Q &q, u64 *headw, uint32_t *out, uint32_t k, uint32_t limit, bool *timed_out,
+		const LG *log)
 {
 	*timed_out = false;
 	for (uint32_t it = 0; it < limit; it++) {
 		const u64 hd = O::ld(headw);
 		uint32_t cur = tw_idx(hd), r = 0;
+		if (log) {
+			const u64 l0 = O::ld(q.link(cur));
+			uint32_t nh = 0;
+			r = iq_chain_from_log<O>(q, log, cur, l0, out, k, &nh);
+			if (r) {
+				if (O::cas(headw, hd, tw_make(tw_tag(hd) + 1u, nh)) == hd)
+					return r;
+				O::pause(it);
+				continue;
+			}
+		}
 		while (r < k) {
 			const uint32_t nx = tw_idx(O::ld(q.link(cur)));
 			if (nx == 0)

@@ -19,7 +19,13 @@
  *     than three times, as the reference's queue tests shuffle items
  *     (dequeue -> enqueue), so items leave and re-enter the queue.
  *
- *   queue_harness clq|iq THREADS CHAINS MAX_CHAIN DEQ_BATCH DELAY_PROB SEED [PRODUCERS [RECYCLE]]
+ *   - the chain log: with LOG_RECORDS > 0 every chain appended (of 3 or
+ *     more items for the pointer queue, 2 or more for the indexed one) is
+ *     recorded in a log of that many records, reused round robin (a small
+ *     log is overwritten while its chains are still queued, so dequeues
+ *     meet stale records), and dequeues take chains from their records.
+ *
+ *   queue_harness clq|iq THREADS CHAINS MAX_CHAIN DEQ_BATCH DELAY_PROB SEED [PRODUCERS [RECYCLE [LOG_RECORDS]]]
  *
  * PRODUCERS of the threads (default half) append CHAINS fresh chains of
  * 1..MAX_CHAIN items each; the rest take batches of 1..DEQ_BATCH until
@@ -102,6 +108,25 @@ struct LinkAtItem {
 const uint32_t LIMIT = 1u << 18;
 const uint32_t HOPS = 3;
 
+/* The chain log: records of 32 items, reused modulo the record count. */
+struct HostLog {
+	std::vector<u64> clq;
+	std::vector<uint32_t> iq;
+	uint32_t mask = 0;
+	std::atomic<uint32_t> next{0};
+	u64 clq_item(uint32_t recno, uint32_t j) const
+	{
+		return __atomic_load_n(&clq[(size_t)(recno & mask) * 32 + j], __ATOMIC_RELAXED);
+	}
+	uint32_t iq_item(uint32_t recno, uint32_t j) const
+	{
+		return __atomic_load_n(&iq[(size_t)(recno & mask) * 32 + j], __ATOMIC_RELAXED);
+	}
+	uint32_t take() { return next.fetch_add(1) & kma_q::LOG_RECNO_MASK; }
+};
+HostLog g_log;
+const HostLog *log_ptr() { return g_log.mask || !g_log.clq.empty() || !g_log.iq.empty() ? &g_log : nullptr; }
+
 struct Result {
 	uint64_t enq = 0, deq = 0, left = 0, bad = 0, order = 0, timeouts = 0;
 };
@@ -152,12 +177,20 @@ void run_clq(int threads, int chains, int maxc, int batch, double recycle, uint6
 	std::atomic<int> producing{np};
 	Book bk(items.size(), (uint64_t)items.size() * HOPS);
 	auto append = [&](Item **v, int len, uint32_t owner, uint32_t &seq) {
+		const bool logged = log_ptr() && len >= 3;
+		const uint32_t recno = logged ? g_log.take() : 0;
 		for (int j = 0; j < len; j++) {
 			v[j]->st.owner = owner;
 			v[j]->st.seq = seq++;
 			v[j]->st.hops++;
 			__atomic_fetch_add(&bk.appends[(size_t)(v[j] - items.data())], 1, __ATOMIC_RELAXED);
-			__atomic_store_n(&v[j]->next, j + 1 < len ? (u64)v[j + 1] : 0ull, __ATOMIC_RELAXED);
+			u64 link = j + 1 < len ? (u64)v[j + 1] : 0ull;
+			if (logged) {
+				__atomic_store_n(&g_log.clq[(size_t)(recno & g_log.mask) * 32 + j], (u64)v[j], __ATOMIC_RELAXED);
+				link |= j == 0 ? kma_q::clq_mark_first(recno, (uint32_t)len)
+					       : (j == 1 ? kma_q::clq_mark_second(recno) : 0ull);
+			}
+			__atomic_store_n(&v[j]->next, link, __ATOMIC_RELAXED);
 		}
 		if (!kma_q::clq_append<HostOps, LinkAtItem>(&q[0], &q[1], (u64)v[0], (u64)v[len - 1], LIMIT))
 			bk.tmo++;
@@ -187,7 +220,8 @@ void run_clq(int threads, int chains, int maxc, int batch, double recycle, uint6
 			bool done = producing.load() == 0;
 			bool to = false;
 			uint32_t k = 1 + (uint32_t)(rnd() % batch);
-			uint32_t r = kma_q::clq_dequeue_n<HostOps, LinkAtItem>(&q[0], &q[1], out.data(), k, LIMIT, &to);
+			uint32_t r = kma_q::clq_dequeue_n<HostOps, LinkAtItem>(&q[0], &q[1], out.data(), k, LIMIT, &to,
+									       log_ptr());
 			if (to)
 				bk.tmo++;
 			back.clear();
@@ -219,7 +253,7 @@ void run_clq(int threads, int chains, int maxc, int batch, double recycle, uint6
 	uint64_t left = 0, bad = bk.deq.load() > bk.cap ? 1 : 0;
 	u64 lastp = 0;
 	for (u64 p = kma_q::qp_ptr(q[0]); p && p != kma_q::POISON && left <= items.size();
-	     p = reinterpret_cast<Item *>(p)->next) {
+	     p = kma_q::qp_ptr(reinterpret_cast<Item *>(p)->next)) {
 		bk.takes[(size_t)(reinterpret_cast<Item *>(p) - items.data())]++;
 		left++;
 		lastp = p;
@@ -263,12 +297,17 @@ void run_iq(int threads, int chains, int maxc, int batch, double recycle, uint64
 	Book bk(n + 2, (n + 1) * HOPS);
 	bk.appends[1] = 1; /* the initial dummy counts as appended */
 	auto append = [&](const uint32_t *v, int len, uint32_t owner, uint32_t &seq) {
+		const bool logged = log_ptr() && len >= 2;
+		const uint32_t recno = logged ? g_log.take() : 0;
 		for (int j = 0; j < len; j++) {
 			st[v[j]].owner = owner;
 			st[v[j]].seq = seq++;
 			st[v[j]].hops++;
 			__atomic_fetch_add(&bk.appends[v[j]], 1, __ATOMIC_RELAXED);
-			kma_q::iq_set_link<HostOps>(q, v[j], j + 1 < len ? v[j + 1] : 0u);
+			if (logged)
+				__atomic_store_n(&g_log.iq[(size_t)(recno & g_log.mask) * 32 + j], v[j], __ATOMIC_RELAXED);
+			kma_q::iq_set_link<HostOps>(q, v[j], j + 1 < len ? v[j + 1] : 0u,
+						    logged && j == 0 ? kma_q::iq_log_tag(recno, (uint32_t)len) : 0u);
 		}
 		kma_q::iq_append<HostOps>(q, &ends[1], v[0], v[len - 1]);
 		bk.enq += len;
@@ -296,7 +335,7 @@ void run_iq(int threads, int chains, int maxc, int batch, double recycle, uint64
 			bool done = producing.load() == 0;
 			bool to = false;
 			uint32_t k = 1 + (uint32_t)(rnd() % batch);
-			uint32_t r = kma_q::iq_dequeue_n<HostOps>(q, &ends[0], out.data(), k, LIMIT, &to);
+			uint32_t r = kma_q::iq_dequeue_n<HostOps>(q, &ends[0], out.data(), k, LIMIT, &to, log_ptr());
 			if (to)
 				bk.tmo++;
 			back.clear();
@@ -348,9 +387,9 @@ void run_iq(int threads, int chains, int maxc, int batch, double recycle, uint64
 
 int main(int argc, char **argv)
 {
-	if (argc < 8 || argc > 10) {
-		fprintf(stderr, "usage: %s clq|iq THREADS CHAINS MAX_CHAIN DEQ_BATCH DELAY_PROB SEED [PRODUCERS [RECYCLE]]\n",
-			argv[0]);
+	if (argc < 8 || argc > 11) {
+		fprintf(stderr, "usage: %s clq|iq THREADS CHAINS MAX_CHAIN DEQ_BATCH DELAY_PROB SEED "
+			"[PRODUCERS [RECYCLE [LOG_RECORDS]]]\n", argv[0]);
 		return 2;
 	}
 	const bool clq = strcmp(argv[1], "clq") == 0;
@@ -360,6 +399,14 @@ int main(int argc, char **argv)
 	if (argc >= 9)
 		g_producers = atoi(argv[8]);
 	const double recycle = argc >= 10 ? atof(argv[9]) : 0.5;
+	const uint32_t log_records = argc >= 11 ? (uint32_t)strtoul(argv[10], NULL, 0) : 0u;
+	if (log_records) {
+		if (log_records & (log_records - 1))
+			return 2; /* a power of two */
+		g_log.mask = log_records - 1;
+		g_log.clq.assign((size_t)log_records * 32, 0);
+		g_log.iq.assign((size_t)log_records * 32, 0);
+	}
 	if (threads < 1 || chains < 1 || maxc < 1 || batch < 1)
 		return 2;
 	Result R;
@@ -370,10 +417,10 @@ int main(int argc, char **argv)
 		run_iq(threads, chains, maxc, batch, recycle, seed, R);
 	double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 	const bool ok = R.bad == 0 && R.order == 0 && R.timeouts == 0;
-	printf("{\"queue\": \"%s\", \"threads\": %d, \"appended\": %llu, \"taken\": %llu, \"left\": %llu, "
+	printf("{\"queue\": \"%s\", \"log_records\": %u, \"threads\": %d, \"appended\": %llu, \"taken\": %llu, \"left\": %llu, "
 	       "\"conservation_faults\": %llu, \"order_faults\": %llu, \"timeouts\": %llu, \"delays\": %llu, "
 	       "\"seconds\": %.3f, \"ok\": %s}\n",
-	       clq ? "clq" : "iq", threads, (unsigned long long)R.enq, (unsigned long long)R.deq,
+	       clq ? "clq" : "iq", log_records, threads, (unsigned long long)R.enq, (unsigned long long)R.deq,
 	       (unsigned long long)R.left, (unsigned long long)R.bad, (unsigned long long)R.order,
 	       (unsigned long long)R.timeouts, (unsigned long long)g_delays.load(), s, ok ? "true" : "false");
 	return ok ? 0 : 1;

@@ -25,14 +25,20 @@ ORACLE = os.path.join(ROOT, "oracle")
 HARNESS = os.path.join(ORACLE, "queue_harness")
 ALGO = os.path.join(ROOT, "include", "kma_queue_algo.cuh")
 
-# threads chains max_chain deq_batch delay_prob seed producers recycle
+# threads chains max_chain deq_batch delay_prob seed producers recycle log_records
 CONFIGS = [
-    "8 20000 1 1 0.01 1 1 0.5",      # single items, one producer: the queue is mostly empty
-    "8 20000 4 4 0.01 2 2 0.5",
-    "8 5000 32 32 0.02 3 4 0.5",     # warp-sized chains and batches, many delayed appends
-    "8 3000 32 32 0.002 4 4 0.9",
-    "8 40000 32 32 0.0005 5 4 0",    # no recycling: plain producer/consumer
-    "3 20000 8 8 0.01 6 1 0.5",
+    "8 20000 1 1 0.01 1 1 0.5 0",      # single items, one producer: the queue is mostly empty
+    "8 20000 4 4 0.01 2 2 0.5 0",
+    "8 5000 32 32 0.02 3 4 0.5 0",     # warp-sized chains and batches, many delayed appends
+    "8 3000 32 32 0.002 4 4 0.9 0",
+    "8 40000 32 32 0.0005 5 4 0 0",    # no recycling: plain producer/consumer
+    "3 20000 8 8 0.01 6 1 0.5 0",
+    # with a chain log: large (records outlive their chains), and small
+    # (records overwritten while their chains are queued: stale records)
+    "8 5000 32 32 0.02 7 4 0.5 65536",
+    "8 5000 32 32 0.02 8 4 0.5 8",
+    "8 20000 8 8 0.01 9 2 0.5 2",
+    "8 40000 32 32 0.0005 10 4 0 1024",
 ]
 
 
@@ -81,6 +87,11 @@ MUTANTS = {
                               "\t\tif (true) { O::st(tailw, 0ull);"),
     # move the indexed queue's head with a plain store: two dequeuers take
     # the same items
+    # take a chain from a log record without checking that the record's
+    # first item is the head: a stale record hands out other items
+    "iq_log_first_unchecked": ("iq", "8 20000 8 8 0.01 2 2 0.5 2",
+                               "\tif (out[0] != h0 || (len > 1 && m > 1",
+                               "\tif ((len > 1 && m > 1"),
     "iq_head_store": ("iq", "8 20000 4 4 0.01 2 2 0.5",
                       "\t\tif (O::cas(headw, hd, tw_make(tw_tag(hd) + 1u, cur)) == hd)\n\t\t\treturn r;",
                       "\t\tO::st(headw, tw_make(tw_tag(hd) + 1u, cur));\n\t\treturn r;"),
