@@ -103,6 +103,44 @@ struct gpu_ops {
 } /* namespace kma_detail */
 
 /* ================================================================== */
+/* chain log (optional, for the warp forms of both queues)             */
+/* ================================================================== */
+/*
+ * A log of `mask + 1` records (a power of two), reused round robin.  A
+ * warp that appends a chain of its items (kma_clqueue_enqueue_warp: 3 or
+ * more items; kma_iqueue_enqueue_warp_shard: 2 or more) writes the items
+ * into the next record and marks the chain's first link(s) with the
+ * record's number; a warp dequeue that finds a marked chain at the head
+ * checks the record against the queue's links with independent loads and
+ * takes the chain at once instead of walking it link by link (the
+ * algorithm and its checks: kma_queue_algo.cuh).  Records are only hints:
+ * a stale or overwritten one fails the check and the dequeue walks.  One
+ * log may serve any number of queues of one kind.  No counterpart in the
+ * reference.
+ */
+struct kma_chain_log {
+	unsigned long long *rec; /* [mask + 1][32] pointers, or [mask + 1][64] u32 indices (first 32 used) */
+	unsigned int *next;      /* record counter, a line of its own */
+	uint32_t mask;
+	uint32_t pad;
+
+	__device__ __forceinline__ unsigned long long clq_item(uint32_t recno, uint32_t j) const
+	{
+		return kma_detail::ld_relaxed64(&rec[(size_t)(recno & mask) * 32 + j]);
+	}
+	__device__ __forceinline__ uint32_t iq_item(uint32_t recno, uint32_t j) const
+	{
+		return kma_detail::ld_relaxed(reinterpret_cast<const uint32_t *>(&rec[(size_t)(recno & mask) * 32]) + j);
+	}
+	__device__ __forceinline__ uint32_t take() { return atomicAdd(next, 1u) & kma_q::LOG_RECNO_MASK; }
+	__device__ __forceinline__ unsigned long long *clq_slot(uint32_t recno) { return &rec[(size_t)(recno & mask) * 32]; }
+	__device__ __forceinline__ uint32_t *iq_slot(uint32_t recno)
+	{
+		return reinterpret_cast<uint32_t *>(&rec[(size_t)(recno & mask) * 32]);
+	}
+};
+
+/* ================================================================== */
 /* kma_clqueue: intrusive pointer FIFO (clQueue.cl:27-118)             */
 /* ================================================================== */
 /*
@@ -204,7 +242,8 @@ __device__ inline unsigned long long clq_dequeue(kma_clqueue *q, uint32_t *err, 
 {
 	unsigned long long out = 0;
 	bool timed_out = false;
-	if (kma_q::clq_dequeue_n<gpu_ops, L>(&q->head, &q->tail, &out, 1, spin_limit, &timed_out))
+	if (kma_q::clq_dequeue_n<gpu_ops, L>(&q->head, &q->tail, &out, 1, spin_limit, &timed_out,
+					      (const kma_chain_log *)nullptr))
 		return out;
 	if (timed_out)
 		flag_err(err, KMA_ERR_TIMEOUT);
@@ -215,7 +254,7 @@ template <class L>
 __device__ __forceinline__ unsigned long long clq_next(unsigned long long p)
 {
 	unsigned long long n = *(const volatile unsigned long long *)L::at(p);
-	return n == KMA_Q_POISON ? 0ull : n;
+	return n == KMA_Q_POISON ? 0ull : qp_ptr(n); /* a logged chain marks the top bits */
 }
 
 /* Lanes grouped by key: this lane's group (lanes with the same key among
@@ -258,11 +297,12 @@ __device__ __forceinline__ kma_clqueue_item *kma_clqueue_dequeue(kma_clqueue *q,
 /* Warp form of enqueue: every calling lane appends its own item (NULL: no
  * item) to its own queue (lanes may name different queues).  The items of
  * one queue are linked in lane order and appended as one chain with one
- * exchange of its tail, so they come out in lane order, together.  Returns
- * what kma_clqueue_enqueue would for the lane's item (1, or 0 for a
- * refused item or an expired wait).  No counterpart in the reference. */
+ * exchange of its tail, so they come out in lane order, together; with a
+ * chain log, chains of 3 or more items are recorded in it.  Returns what
+ * kma_clqueue_enqueue would for the lane's item (1, or 0 for a refused
+ * item or an expired wait).  No counterpart in the reference. */
 __device__ inline int kma_clqueue_enqueue_warp(kma_clqueue *q, kma_clqueue_item *item, uint32_t *err = nullptr,
-		uint32_t spin_limit = KMA_STRUCT_SPIN)
+		uint32_t spin_limit = KMA_STRUCT_SPIN, kma_chain_log *log = nullptr)
 {
 	using namespace kma_detail;
 	const uint32_t active = __activemask();
@@ -272,10 +312,22 @@ __device__ inline int kma_clqueue_enqueue_warp(kma_clqueue *q, kma_clqueue_item 
 	const lane_group gp = group_by(active, lane, ok ? (unsigned long long)q : ~0ull);
 	const unsigned long long nip = __shfl_sync(active, ip, gp.next);
 	const unsigned long long lip = __shfl_sync(active, ip, gp.last);
+	/* a chain of 3 or more: its record number, taken by the first lane */
+	const bool logged = ok && log && gp.size >= 3;
+	uint32_t recno = 0;
+	if (logged && lane == gp.first)
+		recno = log->take();
+	recno = __shfl_sync(active, recno, gp.first);
 	if (ok) {
-		st_relaxed64(clq_link_head::at(ip), gp.next != lane ? nip : 0ull);
-		/* every lane's link is visible before the first lane's exchange
-		 * publishes the chain */
+		unsigned long long link = gp.next != lane ? nip : 0ull;
+		if (logged) {
+			log->clq_slot(recno)[gp.rank] = ip;
+			link |= gp.rank == 0 ? kma_q::clq_mark_first(recno, gp.size)
+					     : (gp.rank == 1 ? kma_q::clq_mark_second(recno) : 0ull);
+		}
+		st_relaxed64(clq_link_head::at(ip), link);
+		/* every lane's link and record entry is visible before the first
+		 * lane's exchange publishes the chain */
 		__threadfence();
 	}
 	__syncwarp(active);
@@ -291,10 +343,11 @@ __device__ inline int kma_clqueue_enqueue_warp(kma_clqueue *q, kma_clqueue_item 
 
 /* Warp form of dequeue: every calling lane takes one item from its own
  * queue (NULL q: none).  The lanes of one queue take consecutive items
- * under one hold of its head, in lane order; lanes left over when the
- * queue runs empty get NULL.  No counterpart in the reference. */
+ * under one hold of its head, in lane order (a logged chain at the head
+ * in one step); lanes left over when the queue runs empty get NULL.  No
+ * counterpart in the reference. */
 __device__ inline kma_clqueue_item *kma_clqueue_dequeue_warp(kma_clqueue *q, uint32_t *err = nullptr,
-		uint32_t spin_limit = KMA_STRUCT_SPIN)
+		uint32_t spin_limit = KMA_STRUCT_SPIN, const kma_chain_log *log = nullptr)
 {
 	using namespace kma_detail;
 	const uint32_t active = __activemask();
@@ -311,7 +364,7 @@ __device__ inline kma_clqueue_item *kma_clqueue_dequeue_warp(kma_clqueue *q, uin
 		if (more && lane == gp.first) {
 			bool timed_out = false;
 			r = kma_q::clq_dequeue_n<gpu_ops, clq_link_head>(&q->head, &q->tail, out, gp.size - served,
-									 spin_limit, &timed_out);
+									 spin_limit, &timed_out, log);
 			if (timed_out)
 				flag_err(err, KMA_ERR_TIMEOUT);
 		}
@@ -383,6 +436,7 @@ struct __align__(128) kma_iqueue {
 	uint32_t nshards;
 	uint32_t spin_limit;
 	uint32_t err;
+	kma_chain_log *log;  /* chain log of the warp forms, or NULL */
 };
 
 namespace kma_detail {
@@ -458,7 +512,8 @@ __device__ inline void *kma_iqueue_dequeue_shard(kma_iqueue *q, uint32_t shard)
 	for (uint32_t k = 0; k < 2; k++) {
 		uint32_t idx = 0;
 		bool timed_out = false;
-		if (!kma_q::iq_dequeue_n<gpu_ops>(L, &q->ends[2 * shard].v, &idx, 1, q->spin_limit, &timed_out)) {
+		if (!kma_q::iq_dequeue_n<gpu_ops>(L, &q->ends[2 * shard].v, &idx, 1, q->spin_limit, &timed_out,
+						  (const kma_chain_log *)nullptr)) {
 			if (timed_out)
 				atomicOr(&q->err, KMA_ERR_TIMEOUT);
 			return nullptr;
@@ -481,8 +536,9 @@ __device__ __forceinline__ void *kma_iqueue_dequeue(kma_iqueue *q)
 
 /* Warp form of enqueue on each lane's shard (NULL item: none): the items
  * of one shard are linked in lane order and appended as one chain with
- * one exchange of its tail.  1 per appended item, 0 for an item outside
- * the array.  No counterpart in the reference. */
+ * one exchange of its tail (recorded in the queue's chain log, if it has
+ * one, from 2 items).  1 per appended item, 0 for an item outside the
+ * array.  No counterpart in the reference. */
 __device__ inline int kma_iqueue_enqueue_warp_shard(kma_iqueue *q, void *item, uint32_t shard)
 {
 	using namespace kma_detail;
@@ -494,8 +550,18 @@ __device__ inline int kma_iqueue_enqueue_warp_shard(kma_iqueue *q, void *item, u
 	const uint32_t nidx = __shfl_sync(active, idx, gp.next);
 	const uint32_t lidx = __shfl_sync(active, idx, gp.last);
 	const iq_links L{q};
+	/* a chain of 2 or more in a queue with a chain log: its record */
+	kma_chain_log *log = q->log;
+	const bool logged = ok && log && gp.size >= 2;
+	uint32_t recno = 0;
+	if (logged && lane == gp.first)
+		recno = log->take();
+	recno = __shfl_sync(active, recno, gp.first);
 	if (ok) {
-		kma_q::iq_set_link<gpu_ops>(L, idx, gp.next != lane ? nidx : 0u);
+		if (logged)
+			log->iq_slot(recno)[gp.rank] = idx;
+		kma_q::iq_set_link<gpu_ops>(L, idx, gp.next != lane ? nidx : 0u,
+					    logged && gp.rank == 0 ? kma_q::iq_log_tag(recno, gp.size) : 0u);
 		/* every lane's link is visible before the first lane's exchange
 		 * publishes the chain */
 		__threadfence();
@@ -525,7 +591,7 @@ __device__ inline void *kma_iqueue_dequeue_warp_shard(kma_iqueue *q, uint32_t sh
 		if (more && lane == gp.first) {
 			bool timed_out = false;
 			r = kma_q::iq_dequeue_n<gpu_ops>(L, &q->ends[2 * shard].v, out, gp.size - served, q->spin_limit,
-							 &timed_out);
+							 &timed_out, (const kma_chain_log *)q->log);
 			if (timed_out)
 				atomicOr(&q->err, KMA_ERR_TIMEOUT);
 			/* internal dummies leave silently */

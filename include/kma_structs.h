@@ -134,13 +134,31 @@ int kma_clarraylist_replay_host(kma_heap_t kma, kma_pma_t pma, uint32_t obj_size
 int kma_clarraylist_group_host(kma_heap_t kma, kma_pma_t pma, uint32_t obj_size,
 			       const uint32_t *objs, uint32_t n, int mode, int64_t *out);
 
+/* ---- chain log (kma_structs.cuh) ----------------------------------------- */
+/* A log of `records` (a power of two, at most 2^25) chain records for the
+ * warp forms of the queues: warp enqueues record each chain's items, warp
+ * dequeues take a recorded chain at the head in one step instead of
+ * walking it.  256 bytes per record; records are reused round robin and
+ * are only hints (checked against the queue before use), so any size is
+ * correct and a size at least the number of chains queued at once is
+ * fastest.  No counterpart in the reference. */
+typedef struct kma_chain_log_s *kma_chain_log_t;
+struct kma_chain_log;
+int kma_chain_log_create(uint32_t records, int device, void *stream, kma_chain_log_t *out);
+int kma_chain_log_destroy(kma_chain_log_t l);
+/* struct kma_chain_log* to pass to kma_clqueue_enqueue_warp / _dequeue_warp */
+struct kma_chain_log *kma_chain_log_device_ptr(kma_chain_log_t l);
+/* Attach a log to an indexed queue's warp forms (NULL detaches). */
+int kma_iqueue_set_chain_log(kma_iqueue_t q, kma_chain_log_t l, void *stream);
+
 /* ---- concurrent microbenchmarks -------------------------------------- */
 #define KMA_C3_CLQUEUE 0
 #define KMA_C3_IQUEUE 1
 /* or'ed into the kind: every enqueue and dequeue through the warp forms
  * (kma_clqueue_enqueue_warp / _dequeue_warp, kma_iqueue_enqueue_warp_shard
  * / _dequeue_warp_shard): a warp's items for one queue go in as one chain
- * and its dequeues take consecutive items together */
+ * and its dequeues take consecutive items together; the queues get a
+ * chain log of one record per 16 payloads (a power of two) */
 #define KMA_C3_WARP 0x100
 
 typedef struct kma_c3_queue_stats {

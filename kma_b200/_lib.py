@@ -170,6 +170,10 @@ SIGNATURES = [
     ("kma_clqueue_device_ptr", c_void_p, [c_void_p]),
     ("kma_iqueue_create", c_int, [c_void_p, c_uint32, c_uint32, c_void_p, c_uint32, c_int, c_void_p,
                                   POINTER(c_void_p)]),
+    ("kma_chain_log_create", c_int, [c_uint32, c_int, c_void_p, POINTER(c_void_p)]),
+    ("kma_chain_log_destroy", c_int, [c_void_p]),
+    ("kma_chain_log_device_ptr", c_void_p, [c_void_p]),
+    ("kma_iqueue_set_chain_log", c_int, [c_void_p, c_void_p, c_void_p]),
     ("kma_iqueue_destroy", c_int, [c_void_p]),
     ("kma_iqueue_device_ptr", c_void_p, [c_void_p]),
     ("kma_iqueue_error_flags", c_int, [c_void_p, c_void_p, POINTER(c_uint32), c_int]),

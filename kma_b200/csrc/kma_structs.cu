@@ -24,6 +24,11 @@ struct kma_iqueue_s {
 	void *mem;
 	kma_iqueue *dq;
 };
+struct kma_chain_log_s {
+	int device;
+	void *mem;
+	kma_chain_log *dl;
+};
 struct kma_cltree_s {
 	int device;
 	kma_cltree *dt;
@@ -451,6 +456,74 @@ extern "C" int kma_iqueue_replay_host(uint32_t n_items, uint32_t stride_l2, cons
 }
 
 /* ------------------------------------------------------------------ */
+/* chain log                                                           */
+/* ------------------------------------------------------------------ */
+
+extern "C" int kma_chain_log_create(uint32_t records, int device, void *stream, kma_chain_log_t *out)
+{
+	if (!out)
+		return KMA_EINVAL;
+	*out = NULL;
+	if (records == 0 || (records & (records - 1)) || records > (1u << 25))
+		return KMA_EINVAL;
+	kma_device_guard g(device);
+	if (!g.ok)
+		return KMA_ENODEV;
+	kma_chain_log_s *l = (kma_chain_log_s *)calloc(1, sizeof(*l));
+	if (!l)
+		return KMA_ENOMEM;
+	l->device = current_device();
+	/* header line, counter line, then the records (zeroed: an entry is 0
+	 * until a chain fills it) */
+	const size_t hdr = 256, bytes = hdr + (size_t)records * 256;
+	if (cudaMalloc(&l->mem, bytes) != cudaSuccess) {
+		cudaGetLastError();
+		free(l);
+		return KMA_ENOMEM;
+	}
+	l->dl = (kma_chain_log *)l->mem;
+	kma_chain_log hl;
+	memset(&hl, 0, sizeof(hl));
+	hl.rec = (unsigned long long *)((unsigned char *)l->mem + hdr);
+	hl.next = (unsigned int *)((unsigned char *)l->mem + 128);
+	hl.mask = records - 1;
+	cudaStream_t st = kma_stream(stream);
+	int rc = KMA_OK;
+	if (cudaMemsetAsync(l->mem, 0, bytes, st) != cudaSuccess)
+		rc = KMA_ECUDA;
+	if (rc == KMA_OK)
+		rc = put_sync(l->dl, &hl, sizeof(hl), st);
+	if (rc != KMA_OK) {
+		cudaFree(l->mem);
+		free(l);
+		return rc;
+	}
+	*out = l;
+	return KMA_OK;
+}
+
+extern "C" int kma_chain_log_destroy(kma_chain_log_t l)
+{
+	if (!l)
+		return KMA_EINVAL;
+	kma_device_guard g(l->device);
+	cudaError_t e = cudaFree(l->mem);
+	free(l);
+	return e == cudaSuccess ? KMA_OK : KMA_ECUDA;
+}
+
+extern "C" struct kma_chain_log *kma_chain_log_device_ptr(kma_chain_log_t l) { return l ? l->dl : NULL; }
+
+extern "C" int kma_iqueue_set_chain_log(kma_iqueue_t q, kma_chain_log_t l, void *stream)
+{
+	if (!q)
+		return KMA_EINVAL;
+	kma_device_guard g(q->device);
+	kma_chain_log *p = l ? l->dl : NULL;
+	return put_sync(&q->dq->log, &p, sizeof(p), kma_stream(stream));
+}
+
+/* ------------------------------------------------------------------ */
 /* clTree                                                              */
 /* ------------------------------------------------------------------ */
 
@@ -782,7 +855,7 @@ __device__ __forceinline__ void warp_flush(unsigned long long *dst, unsigned lon
  * [8] walk failures */
 template <bool WARP>
 __global__ void k_c3_clq_enq(unsigned char *qs, uint32_t shards, unsigned char *items, uint32_t per_thread,
-		uint32_t n, uint64_t seed, unsigned long long *acc, uint32_t *err)
+		uint32_t n, uint64_t seed, unsigned long long *acc, uint32_t *err, kma_chain_log *log)
 {
 	uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
 	unsigned long long c = 0, x = 0, s = 0;
@@ -796,7 +869,7 @@ __global__ void k_c3_clq_enq(unsigned char *qs, uint32_t shards, unsigned char *
 		uint32_t pay = i < n ? perm_u32(i, n, seed) : 0u;
 		if (it)
 			*(uint32_t *)(it + 8) = pay;
-		int ok = WARP ? kma_clqueue_enqueue_warp(q, (kma_clqueue_item *)it, err)
+		int ok = WARP ? kma_clqueue_enqueue_warp(q, (kma_clqueue_item *)it, err, KMA_STRUCT_SPIN, log)
 			      : kma_clqueue_enqueue(q, (kma_clqueue_item *)it, err);
 		if (ok) {
 			c++;
@@ -809,14 +882,15 @@ __global__ void k_c3_clq_enq(unsigned char *qs, uint32_t shards, unsigned char *
 
 template <bool WARP>
 __global__ void k_c3_clq_deq(unsigned char *qs, uint32_t shards, uint32_t per_thread, uint32_t threads,
-		unsigned long long *acc, uint32_t *err)
+		unsigned long long *acc, uint32_t *err, const kma_chain_log *log)
 {
 	uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
 	unsigned long long c = 0, x = 0, s = 0, e = 0;
 	if (WARP || t < threads) {
 		kma_clqueue *q = t < threads ? (kma_clqueue *)(qs + (size_t)(t % shards) * 128) : nullptr;
 		for (uint32_t k = 0; k < per_thread; k++) {
-			kma_clqueue_item *it = WARP ? kma_clqueue_dequeue_warp(q, err) : kma_clqueue_dequeue(q, err);
+			kma_clqueue_item *it = WARP ? kma_clqueue_dequeue_warp(q, err, KMA_STRUCT_SPIN, log)
+						    : kma_clqueue_dequeue(q, err);
 			if (!q)
 				continue;
 			if (!it) {
@@ -993,27 +1067,41 @@ extern "C" int kma_c3_queue_run(int kind, uint32_t threads, uint32_t per_thread,
 	uint32_t blocks = (threads + 255) / 256;
 	int rc = KMA_OK;
 	kma_iqueue_t iq = NULL;
-	if (kind == KMA_C3_CLQUEUE) {
+	/* warp forms: a chain log of one record per 16 payloads (every chain
+	 * of this run keeps its record: chains hold up to 32 payloads) */
+	kma_chain_log_t log = NULL;
+	if (warp) {
+		uint32_t rec = 1;
+		while (rec < n / 16 && rec < (1u << 25))
+			rec <<= 1;
+		rc = kma_chain_log_create(rec, -1, NULL, &log);
+	}
+	if (rc != KMA_OK) {
+		/* no log: nothing ran */
+	} else if (kind == KMA_C3_CLQUEUE) {
 		unsigned char *qs = b.alloc<unsigned char>((size_t)shards * 128);
 		if (!qs)
 			rc = KMA_ENOMEM;
 		if (rc == KMA_OK) {
 			cudaMemset(qs, 0, (size_t)shards * 128);
 			cudaEventRecord(e0);
+			kma_chain_log *dl = kma_chain_log_device_ptr(log);
 			if (warp)
-				k_c3_clq_enq<true><<<blocks, 256>>>(qs, shards, items, per_thread, n, seed, acc, err);
+				k_c3_clq_enq<true><<<blocks, 256>>>(qs, shards, items, per_thread, n, seed, acc, err, dl);
 			else
-				k_c3_clq_enq<false><<<blocks, 256>>>(qs, shards, items, per_thread, n, seed, acc, err);
+				k_c3_clq_enq<false><<<blocks, 256>>>(qs, shards, items, per_thread, n, seed, acc, err, dl);
 			cudaEventRecord(e1);
 			if (warp)
-				k_c3_clq_deq<true><<<blocks, 256>>>(qs, shards, per_thread, threads, acc, err);
+				k_c3_clq_deq<true><<<blocks, 256>>>(qs, shards, per_thread, threads, acc, err, dl);
 			else
-				k_c3_clq_deq<false><<<blocks, 256>>>(qs, shards, per_thread, threads, acc, err);
+				k_c3_clq_deq<false><<<blocks, 256>>>(qs, shards, per_thread, threads, acc, err, dl);
 			cudaEventRecord(e2);
 			k_c3_clq_walk<<<(shards + 127) / 128, 128>>>(qs, shards, n, acc);
 		}
 	} else {
 		rc = kma_iqueue_create(items, 4, n + 1, items, shards, -1, NULL, &iq);
+		if (rc == KMA_OK && log)
+			rc = kma_iqueue_set_chain_log(iq, log, NULL);
 		if (rc == KMA_OK) {
 			cudaEventRecord(e0);
 			if (warp)
@@ -1056,6 +1144,8 @@ extern "C" int kma_c3_queue_run(int kind, uint32_t threads, uint32_t per_thread,
 	}
 	if (iq)
 		kma_iqueue_destroy(iq);
+	if (log)
+		kma_chain_log_destroy(log);
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	cudaEventDestroy(e2);

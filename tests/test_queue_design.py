@@ -109,8 +109,16 @@ def test_harness_detects_planted_mistakes(harness, tmp_path, name):
     binary = str(d / "h")
     subprocess.run([os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-pthread", f"-I{d}", "-o", binary,
                     os.path.join(ORACLE, "queue_harness.cpp")], check=True)
-    try:
-        rc, st = run(binary, kind, cfg, timeout=120)
-    except subprocess.TimeoutExpired:
-        return  # a wait that never ends is a detection too
-    assert rc != 0, f"mutant {name} passed unnoticed: {st}"
+    # a fault shows up in most runs, not all: up to four seeds, the first
+    # detection is enough
+    st = {}
+    for seed in range(4):
+        args = cfg.split()
+        args[5] = str(int(args[5]) + 100 * seed)
+        try:
+            rc, st = run(binary, kind, " ".join(args), timeout=120)
+        except subprocess.TimeoutExpired:
+            return  # a wait that never ends is a detection too
+        if rc != 0:
+            return
+    raise AssertionError(f"mutant {name} passed unnoticed: {st}")
