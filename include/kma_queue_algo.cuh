@@ -204,10 +204,6 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 			O::pause(it++);
 			continue;
 		}
-		/* a logged chain at the head: check its record before the hold, so
-		 * the hold lasts only the exchange and the head check */
-		u64 nh = 0;
-		const uint32_t m = clq_chain_from_log<O, L>(log, hp, seen, out, k, &nh);
 		const u64 nx = O::xchg(hl, POISON);
 		if (nx == POISON) {
 			/* another dequeuer holds it, or it left the queue already */
@@ -221,8 +217,12 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 			O::pause(it++);
 			continue;
 		}
-		if (m && nx == seen) {
-			/* nothing moved since the check: the chain's links are those */
+		/* a logged chain at the head: its record, checked against the
+		 * links while the head is held (the items behind a held head
+		 * cannot move), gives the chain without walking it */
+		u64 nh = 0;
+		const uint32_t m = clq_chain_from_log<O, L>(log, hp, nx, out, k, &nh);
+		if (m) {
 			for (uint32_t j = 1; j < m; j++)
 				O::st_rlx(L::at(out[j]), POISON);
 			O::st(headw, qp_next(h, nh));
@@ -346,10 +346,16 @@ KQ_FN uint32_t iq_chain_from_log(const Q &q, const LG *log, uint32_t h0, u64 l0,
 
 /* Dequeue up to k old dummies into out[] (indices, FIFO order).  Returns
  * the number taken: 0 when the dummy has no successor, or (with
- * *timed_out) when the CAS kept losing past `limit` tries.  Reads the
- * chain behind the head first and moves the head past it with one CAS; a
- * head that moved meanwhile fails the CAS (its tag changed) and the walk
- * is retried. */
+ * *timed_out) when the head stayed held past `limit` tries.
+ *
+ * A dequeuer holds the head while it takes its items: the head's tag is
+ * even when free and odd while held (a CAS to tag+1 takes it, the store
+ * of the new head with tag+2 gives it back).  The holder reads the chain
+ * behind the head (from the log, or link by link) and moves the head past
+ * it; others wait reading the head, so a batch's loads are issued by one
+ * dequeuer at a time instead of by every contender.  A holder never waits
+ * for anything, so a hold lasts a few round trips. */
+KQ_FN bool iq_head_held(u64 hd) { return tw_tag(hd) & 1u; }
 template <class O, class Q, class LG>
 KQ_FN uint32_t iq_dequeue_n(const Q &q, u64 *headw, uint32_t *out, uint32_t k, uint32_t limit, bool *timed_out,
 		const LG *log)
@@ -357,33 +363,39 @@ KQ_FN uint32_t iq_dequeue_n(const Q &q, u64 *headw, uint32_t *out, uint32_t k, u
 	*timed_out = false;
 	for (uint32_t it = 0; it < limit; it++) {
 		const u64 hd = O::ld(headw);
+		if (iq_head_held(hd)) {
+			O::pause(it);
+			continue;
+		}
 		uint32_t cur = tw_idx(hd), r = 0;
-		if (log) {
-			const u64 l0 = O::ld(q.link(cur));
-			uint32_t nh = 0;
-			r = iq_chain_from_log<O>(q, log, cur, l0, out, k, &nh);
-			if (r) {
-				if (O::cas(headw, hd, tw_make(tw_tag(hd) + 1u, nh)) == hd)
-					return r;
-				O::pause(it);
-				continue;
-			}
-		}
-		while (r < k) {
-			const uint32_t nx = tw_idx(O::ld(q.link(cur)));
-			if (nx == 0)
-				break;
-			out[r++] = cur;
-			cur = nx;
-		}
-		if (r == 0) {
+		const u64 l0 = O::ld(q.link(cur));
+		if (tw_idx(l0) == 0) {
+			/* only the dummy: empty, if the head is still this one */
 			if (O::ld(headw) == hd)
 				return 0;
 			continue;
 		}
-		if (O::cas(headw, hd, tw_make(tw_tag(hd) + 1u, cur)) == hd)
-			return r;
-		O::pause(it);
+		if (O::cas(headw, hd, tw_make(tw_tag(hd) + 1u, cur)) != hd) {
+			O::pause(it);
+			continue;
+		}
+		/* held: the items behind the head cannot leave the queue */
+		uint32_t nh = 0;
+		if (log)
+			r = iq_chain_from_log<O>(q, log, cur, O::ld(q.link(cur)), out, k, &nh);
+		if (r) {
+			cur = nh;
+		} else {
+			while (r < k) {
+				const uint32_t nx = tw_idx(O::ld(q.link(cur)));
+				if (nx == 0)
+					break;
+				out[r++] = cur;
+				cur = nx;
+			}
+		}
+		O::st(headw, tw_make(tw_tag(hd) + 2u, cur));
+		return r;
 	}
 	*timed_out = true;
 	return 0;
