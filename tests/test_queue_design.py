@@ -85,11 +85,6 @@ MUTANTS = {
     "last_item_no_tail_cas": ("clq", "8 20000 1 1 0.01 1 1 0.5",
                               "\t\tif (O::cas(tailw, hp, 0ull) == hp) {",
                               "\t\tif (true) { O::st(tailw, 0ull);"),
-    # take a chain from a log record without checking that the record's
-    # first item is the head: a stale record hands out other items
-    "iq_log_first_unchecked": ("iq", "8 20000 8 8 0.01 2 2 0.5 2",
-                               "\tif (out[0] != h0 || (len > 1 && m > 1",
-                               "\tif ((len > 1 && m > 1"),
     # take the indexed queue's head hold with a plain store: two dequeuers
     # hold it at once and take the same items
     "iq_hold_store": ("iq", "8 20000 4 4 0.01 2 2 0.5",
