@@ -37,9 +37,12 @@
  * when the queue's current links say exactly what the record says, and
  * walks otherwise.
  *
- * Log policy `LG` (a null pointer: no log) provides the items of record
- * `recno` (records are reused modulo the log's size):
- *   iq_item(recno, j)    index of item j        clq_item(recno, j)   pointer of item j
+ * Log policy `LG` (a null pointer, or the type no_log: no log; `enabled`
+ * false compiles the log code out) provides the slot of record `recno`
+ * (records are reused modulo the log's size):
+ *   iq_record(recno)     32 item indices        clq_record(recno)    32 item pointers
+ *   LG::ld(p)            relaxed load of one entry
+ *   taken(m)             a chain of m items was taken from a record (a count)
  *
  * Policy `O` provides, on 64-bit words:
  *   ld(p)        acquire load        st(p, v)     release store
@@ -81,6 +84,16 @@ const u64 PTR_MASK = (1ull << PTR_BITS) - 1ull;
 const uint32_t LOG_RECNO_MASK = 0x1FFFFFFu;
 const uint32_t LOG_CHAIN_MAX = 32;
 
+/* The log policy of callers without a log: the log code compiles away. */
+struct no_log {
+	static constexpr bool enabled = false;
+	KQ_FN const u64 *clq_record(uint32_t) const { return nullptr; }
+	KQ_FN const uint32_t *iq_record(uint32_t) const { return nullptr; }
+	static KQ_FN u64 ld(const u64 *) { return 0; }
+	static KQ_FN uint32_t ld(const uint32_t *) { return 0; }
+	KQ_FN void taken(uint32_t) const {}
+};
+
 KQ_FN u64 qp_ptr(u64 w) { return w & PTR_MASK; }
 KQ_FN u64 qp_next(u64 w, u64 ptr) { return (((w >> PTR_BITS) + 1ull) << PTR_BITS) | ptr; }
 
@@ -102,6 +115,8 @@ KQ_FN u64 clq_mark_second(uint32_t recno) { return (u64)(recno & 0x7FFFu) << PTR
 template <class O, class L, class LG>
 KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32_t k, u64 *nh)
 {
+	if constexpr (!LG::enabled)
+		return 0;
 	if (!log || !(v & CLQ_LOG) || k == 0)
 		return 0;
 	const uint32_t mark = (uint32_t)(v >> PTR_BITS);
@@ -109,38 +124,59 @@ KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32
 	const u64 second = qp_ptr(v);
 	if (len < 3 || second <= POISON)
 		return 0;
-	const u64 l1 = O::ld(L::at(second));
+	/* relaxed loads, issued back to back into registers: an acquire load,
+	 * or a store of each value before the next load, would make them one
+	 * round trip each, as a walk.  The exchange that took the head
+	 * already ordered the chain's contents before these reads. */
+	const u64 l1 = O::ld_rlx(L::at(second));
 	const uint32_t recno = ((mark & 0x3FFu) << 15) | ((uint32_t)(l1 >> PTR_BITS) & 0x7FFFu);
 	uint32_t m = len < k ? len : k;
-	for (uint32_t j = 0; j < m; j++)
-		out[j] = log->clq_item(recno, j);
-	const u64 after = m < len ? log->clq_item(recno, m) : 0ull;
-	if (out[0] != hp || (m > 1 && out[1] != second) || (m > 2 && out[2] != qp_ptr(l1)))
+	const u64 *rec = log->clq_record(recno);
+	u64 item[LOG_CHAIN_MAX];
+#pragma unroll
+	for (uint32_t j = 0; j < LOG_CHAIN_MAX; j++)
+		item[j] = j <= m && j < len ? LG::ld(rec + j) : 0ull;
+	const u64 after = m < len ? item[m < LOG_CHAIN_MAX ? m : 0] : 0ull;
+	if (item[0] != hp || (m > 1 && item[1] != second) || (m > 2 && item[2] != qp_ptr(l1)))
 		return 0;
 	/* record entries are 0 or item pointers (0 in a slot a chain has not
 	 * filled, or is refilling): none may be followed before it is known
 	 * to be an item */
-	for (uint32_t j = 3; j < m; j++)
-		if (out[j] <= POISON)
-			return 0;
-	u64 nx[LOG_CHAIN_MAX];
-	for (uint32_t j = 2; j < m; j++) /* independent loads */
-		nx[j] = O::ld(L::at(out[j]));
-	for (uint32_t j = 2; j + 1 < m; j++)
-		if (nx[j] == POISON || qp_ptr(nx[j]) != out[j + 1])
-			return 0;
-	u64 next = m == 1 ? second : (m == 2 ? qp_ptr(l1) : nx[m - 1]);
-	if (next == POISON)
+	bool ok = true;
+#pragma unroll
+	for (uint32_t j = 2; j < LOG_CHAIN_MAX; j++)
+		ok &= !(j < m && item[j] <= POISON);
+	if (!ok)
 		return 0;
-	next = qp_ptr(next);
+	/* each item's link must name the next item (for the last one taken:
+	 * the new head) */
+	u64 nxs[LOG_CHAIN_MAX];
+#pragma unroll
+	for (uint32_t j = 2; j < LOG_CHAIN_MAX; j++)
+		nxs[j] = j < m ? O::ld_rlx(L::at(item[j])) : 0ull;
+	u64 last = m == 1 ? second : (m == 2 ? l1 : 0ull);
+#pragma unroll
+	for (uint32_t j = 2; j < LOG_CHAIN_MAX; j++) {
+		if (j + 1 < m)
+			ok &= nxs[j] != POISON && qp_ptr(nxs[j]) == item[j + 1];
+		else if (j + 1 == m)
+			last = nxs[j];
+	}
+	if (!ok || last == POISON)
+		return 0;
+	u64 next = qp_ptr(last);
 	if (m < len) {
-		if (next != after)
+		if (next != after || next == 0)
 			return 0;
 	} else if (next == 0) {
 		/* the chain's last item has no successor yet: it stays, as the head */
-		next = out[m - 1];
+		next = item[(m - 1) & (LOG_CHAIN_MAX - 1)];
 		m--;
 	}
+#pragma unroll
+	for (uint32_t j = 0; j < LOG_CHAIN_MAX; j++)
+		if (j < m)
+			out[j] = item[j];
 	*nh = next;
 	return m;
 }
@@ -192,14 +228,18 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 	*timed_out = false;
 	uint32_t it = 0;
 	while (it < limit) {
-		const u64 h = O::ld(headw);
+		/* waiters poll with relaxed loads: an acquire load also invalidates
+		 * the SM's L1 on the GPU (under contention thousands of waiters
+		 * would keep evicting the holder's local data); the exchange that
+		 * takes the head item is the acquire */
+		const u64 h = O::ld_rlx(headw);
 		const u64 hp = qp_ptr(h);
 		if (hp == 0)
 			return 0;
 		u64 *hl = L::at(hp);
 		/* look before taking: while another dequeuer holds the head item,
 		 * waiters only read its link */
-		const u64 seen = O::ld(hl);
+		const u64 seen = O::ld_rlx(hl);
 		if (seen == POISON) {
 			O::pause(it++);
 			continue;
@@ -223,6 +263,7 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 		u64 nh = 0;
 		const uint32_t m = clq_chain_from_log<O, L>(log, hp, nx, out, k, &nh);
 		if (m) {
+			log->taken(m);
 			for (uint32_t j = 1; j < m; j++)
 				O::st_rlx(L::at(out[j]), POISON);
 			O::st(headw, qp_next(h, nh));
@@ -310,38 +351,74 @@ template <class O, class Q, class LG>
 KQ_FN uint32_t iq_chain_from_log(const Q &q, const LG *log, uint32_t h0, u64 l0, uint32_t *out, uint32_t k,
 		uint32_t *nh)
 {
-	const uint32_t tag = tw_tag(l0);
-	if (!log || !(tag & IQ_LOG) || k == 0)
+	if constexpr (!LG::enabled)
 		return 0;
+	if (!log || k == 0)
+		return 0;
+	/* The head is a dummy when whole chains were taken before: it is the
+	 * last item of the chain before, and the next chain starts at its
+	 * successor.  Take the dummy, then up to k-1 items of that chain. */
+	uint32_t lead = 0;
+	if (!(tw_tag(l0) & IQ_LOG)) {
+		const uint32_t n1 = tw_idx(l0);
+		if (n1 == 0 || k < 2)
+			return 0;
+		lead = h0;
+		h0 = n1;
+		l0 = O::ld_rlx(q.link(n1));
+		k--;
+		if (!(tw_tag(l0) & IQ_LOG))
+			return 0;
+	}
+	const uint32_t tag = tw_tag(l0);
 	const uint32_t len = (tag & 31u) + 1u;
 	const uint32_t recno = (tag >> 5) & LOG_RECNO_MASK;
 	/* the record's items, and the link after each: item j -> item j+1 must
-	 * hold for the items taken and for the one that becomes the head */
+	 * hold for the items taken and for the one that becomes the head.
+	 * Loads into registers, back to back (see clq_chain_from_log). */
 	uint32_t m = len < k ? len : k;
-	for (uint32_t j = 0; j < m; j++)
-		out[j] = log->iq_item(recno, j);
-	const uint32_t after = m < len ? log->iq_item(recno, m) : 0u;
-	if (out[0] != h0 || (len > 1 && m > 1 && out[1] != tw_idx(l0)) || (m == 1 && len > 1 && after != tw_idx(l0)))
+	const uint32_t *rec = log->iq_record(recno);
+	uint32_t item[LOG_CHAIN_MAX];
+#pragma unroll
+	for (uint32_t j = 0; j < LOG_CHAIN_MAX; j++)
+		item[j] = j <= m && j < len ? LG::ld(rec + j) : 0u;
+	const uint32_t after = m < len ? item[m < LOG_CHAIN_MAX ? m : 0] : 0u;
+	if (item[0] != h0 || (m > 1 && item[1] != tw_idx(l0)) || (m == 1 && len > 1 && after != tw_idx(l0)))
 		return 0;
-	uint32_t nx[LOG_CHAIN_MAX];
-	for (uint32_t j = 1; j < m; j++) /* independent loads */
-		nx[j] = tw_idx(O::ld(q.link(out[j])));
-	for (uint32_t j = 1; j + 1 < m; j++)
-		if (nx[j] != out[j + 1])
-			return 0;
-	uint32_t next = m == 1 ? tw_idx(l0) : nx[m - 1];
+	uint32_t nxs[LOG_CHAIN_MAX];
+#pragma unroll
+	for (uint32_t j = 1; j < LOG_CHAIN_MAX; j++)
+		nxs[j] = j < m ? tw_idx(O::ld_rlx(q.link(item[j]))) : 0u;
+	bool ok = true;
+	uint32_t next = m == 1 ? tw_idx(l0) : 0u;
+#pragma unroll
+	for (uint32_t j = 1; j < LOG_CHAIN_MAX; j++) {
+		if (j + 1 < m)
+			ok &= nxs[j] == item[j + 1];
+		else if (j + 1 == m)
+			next = nxs[j];
+	}
+	if (!ok)
+		return 0;
 	if (m < len) {
-		if (next != after)
+		if (next != after || next == 0)
 			return 0;
 	} else if (next == 0) {
 		/* the chain's last item has no successor yet: it stays, as the head */
 		if (m == 1)
 			return 0;
-		next = out[m - 1];
+		next = item[(m - 1) & (LOG_CHAIN_MAX - 1)];
 		m--;
 	}
+	const uint32_t off = lead ? 1u : 0u;
+	if (lead)
+		out[0] = lead;
+#pragma unroll
+	for (uint32_t j = 0; j < LOG_CHAIN_MAX; j++)
+		if (j < m)
+			out[j + off] = item[j];
 	*nh = next;
-	return m;
+	return m + off;
 }
 
 /* Dequeue up to k old dummies into out[] (indices, FIFO order).  Returns
@@ -362,16 +439,18 @@ KQ_FN uint32_t iq_dequeue_n(const Q &q, u64 *headw, uint32_t *out, uint32_t k, u
 {
 	*timed_out = false;
 	for (uint32_t it = 0; it < limit; it++) {
-		const u64 hd = O::ld(headw);
+		/* relaxed polling, as in clq_dequeue_n; the CAS that takes the
+		 * head is the acquire */
+		const u64 hd = O::ld_rlx(headw);
 		if (iq_head_held(hd)) {
 			O::pause(it);
 			continue;
 		}
 		uint32_t cur = tw_idx(hd), r = 0;
-		const u64 l0 = O::ld(q.link(cur));
+		const u64 l0 = O::ld_rlx(q.link(cur));
 		if (tw_idx(l0) == 0) {
 			/* only the dummy: empty, if the head is still this one */
-			if (O::ld(headw) == hd)
+			if (O::ld_rlx(headw) == hd)
 				return 0;
 			continue;
 		}
@@ -381,9 +460,11 @@ KQ_FN uint32_t iq_dequeue_n(const Q &q, u64 *headw, uint32_t *out, uint32_t k, u
 		}
 		/* held: the items behind the head cannot leave the queue */
 		uint32_t nh = 0;
-		if (log)
-			r = iq_chain_from_log<O>(q, log, cur, O::ld(q.link(cur)), out, k, &nh);
+		if constexpr (LG::enabled)
+			if (log)
+				r = iq_chain_from_log<O>(q, log, cur, O::ld(q.link(cur)), out, k, &nh);
 		if (r) {
+			log->taken(r);
 			cur = nh;
 		} else {
 			while (r < k) {

@@ -25,6 +25,9 @@
 #include "kma_queue_algo.cuh"
 
 #define KMA_STRUCT_SPIN (1u << 20)
+#ifndef KMA_QUEUE_PAUSE_MAX_NS
+#define KMA_QUEUE_PAUSE_MAX_NS 4096u
+#endif
 
 namespace kma_detail {
 
@@ -90,13 +93,14 @@ struct gpu_ops {
 		return cas64_acqrel(p, c, v);
 	}
 	/* after `it` fruitless tries: a randomised wait (__nanosleep(t) sleeps
-	 * somewhere in [0, 2t]) of 64 ns doubling per try, at most 4 us, so
-	 * that the waiters on one hot word do not flood its L2 slice with
-	 * requests queued ahead of the holder's */
+	 * somewhere in [0, 2t]) of 64 ns doubling per try, at most
+	 * KMA_QUEUE_PAUSE_MAX_NS, so that the waiters on one hot word do not
+	 * flood its L2 slice with requests queued ahead of the holder's: with
+	 * thousands of waiters one of them still looks soon after a release */
 	static __device__ __forceinline__ void pause(uint32_t it)
 	{
-		const uint32_t t = 64u << (it < 6 ? it : 6);
-		__nanosleep(t);
+		const uint32_t t = 64u << (it < 12 ? it : 12);
+		__nanosleep(t < KMA_QUEUE_PAUSE_MAX_NS ? t : KMA_QUEUE_PAUSE_MAX_NS);
 	}
 };
 
@@ -119,20 +123,29 @@ struct gpu_ops {
  * reference.
  */
 struct kma_chain_log {
+	static constexpr bool enabled = true;
 	unsigned long long *rec; /* [mask + 1][32] pointers, or [mask + 1][64] u32 indices (first 32 used) */
 	unsigned int *next;      /* record counter, a line of its own */
 	uint32_t mask;
 	uint32_t pad;
 
-	__device__ __forceinline__ unsigned long long clq_item(uint32_t recno, uint32_t j) const
+	/* a record's slot; its entries are read with ld (relaxed) */
+	__device__ __forceinline__ const unsigned long long *clq_record(uint32_t recno) const
 	{
-		return kma_detail::ld_relaxed64(&rec[(size_t)(recno & mask) * 32 + j]);
+		return &rec[(size_t)(recno & mask) * 32];
 	}
-	__device__ __forceinline__ uint32_t iq_item(uint32_t recno, uint32_t j) const
+	__device__ __forceinline__ const uint32_t *iq_record(uint32_t recno) const
 	{
-		return kma_detail::ld_relaxed(reinterpret_cast<const uint32_t *>(&rec[(size_t)(recno & mask) * 32]) + j);
+		return reinterpret_cast<const uint32_t *>(&rec[(size_t)(recno & mask) * 32]);
 	}
+	static __device__ __forceinline__ unsigned long long ld(const unsigned long long *p)
+	{
+		return kma_detail::ld_relaxed64(p);
+	}
+	static __device__ __forceinline__ uint32_t ld(const uint32_t *p) { return kma_detail::ld_relaxed(p); }
 	__device__ __forceinline__ uint32_t take() { return atomicAdd(next, 1u) & kma_q::LOG_RECNO_MASK; }
+	/* chains taken from their records (next[1], a count for reports) */
+	__device__ __forceinline__ void taken(uint32_t) const { atomicAdd(next + 1, 1u); }
 	__device__ __forceinline__ unsigned long long *clq_slot(uint32_t recno) { return &rec[(size_t)(recno & mask) * 32]; }
 	__device__ __forceinline__ uint32_t *iq_slot(uint32_t recno)
 	{
@@ -243,7 +256,7 @@ __device__ inline unsigned long long clq_dequeue(kma_clqueue *q, uint32_t *err, 
 	unsigned long long out = 0;
 	bool timed_out = false;
 	if (kma_q::clq_dequeue_n<gpu_ops, L>(&q->head, &q->tail, &out, 1, spin_limit, &timed_out,
-					      (const kma_chain_log *)nullptr))
+					      (const kma_q::no_log *)nullptr))
 		return out;
 	if (timed_out)
 		flag_err(err, KMA_ERR_TIMEOUT);
@@ -481,9 +494,27 @@ __device__ __forceinline__ void *kma_iqueue_item(const kma_iqueue *q, uint32_t i
 
 namespace kma_detail {
 /* the item links of q, as the queue algorithms address them */
+/* The queue's geometry, read once into registers: the queue algorithms'
+ * strong loads and atomics order every later plain load of the queue
+ * struct behind them, so computing each link address from the struct
+ * would put a round trip of its own in front of every link load. */
 struct iq_links {
-	const kma_iqueue *q;
-	__device__ __forceinline__ unsigned long long *link(uint32_t idx) const { return iq_link(q, idx); }
+	unsigned char *base;
+	unsigned long long *dummies;
+	uint32_t stride_l2, capacity, nshards;
+	__device__ __forceinline__ explicit iq_links(const kma_iqueue *q)
+	    : base(q->base), dummies(q->dummies), stride_l2(q->stride_l2), capacity(q->capacity), nshards(q->nshards)
+	{
+	}
+	/* iq_link with the geometry in registers */
+	__device__ __forceinline__ unsigned long long *link(uint32_t idx) const
+	{
+		if (idx == 0)
+			return &dummies[nshards - 1];
+		if (idx > capacity)
+			return &dummies[idx - capacity - 1];
+		return reinterpret_cast<unsigned long long *>(base + ((size_t)(idx - 1) << stride_l2));
+	}
 };
 } /* namespace kma_detail */
 
@@ -495,7 +526,7 @@ __device__ inline int kma_iqueue_enqueue_shard(kma_iqueue *q, void *item, uint32
 	uint32_t idx = iq_idx(q, item);
 	if (idx == 0)
 		return 0;
-	const iq_links L{q};
+	const iq_links L(q);
 	kma_q::iq_set_link<gpu_ops>(L, idx, 0u);
 	/* the link is published by the exchange (acq_rel) that appends it */
 	kma_q::iq_append<gpu_ops>(L, &q->ends[2 * shard + 1].v, idx, idx);
@@ -508,12 +539,12 @@ __device__ inline int kma_iqueue_enqueue_shard(kma_iqueue *q, void *item, uint32
 __device__ inline void *kma_iqueue_dequeue_shard(kma_iqueue *q, uint32_t shard)
 {
 	using namespace kma_detail;
-	const iq_links L{q};
+	const iq_links L(q);
 	for (uint32_t k = 0; k < 2; k++) {
 		uint32_t idx = 0;
 		bool timed_out = false;
 		if (!kma_q::iq_dequeue_n<gpu_ops>(L, &q->ends[2 * shard].v, &idx, 1, q->spin_limit, &timed_out,
-						  (const kma_chain_log *)nullptr)) {
+						  (const kma_q::no_log *)nullptr)) {
 			if (timed_out)
 				atomicOr(&q->err, KMA_ERR_TIMEOUT);
 			return nullptr;
@@ -549,7 +580,7 @@ __device__ inline int kma_iqueue_enqueue_warp_shard(kma_iqueue *q, void *item, u
 	const lane_group gp = group_by(active, lane, ok ? (unsigned long long)shard : ~0ull);
 	const uint32_t nidx = __shfl_sync(active, idx, gp.next);
 	const uint32_t lidx = __shfl_sync(active, idx, gp.last);
-	const iq_links L{q};
+	const iq_links L(q);
 	/* a chain of 2 or more in a queue with a chain log: its record */
 	kma_chain_log *log = q->log;
 	const bool logged = ok && log && gp.size >= 2;
@@ -582,7 +613,7 @@ __device__ inline void *kma_iqueue_dequeue_warp_shard(kma_iqueue *q, uint32_t sh
 	const uint32_t active = __activemask();
 	const uint32_t lane = lane_id();
 	const lane_group gp = group_by(active, lane, want ? (unsigned long long)shard : ~0ull);
-	const iq_links L{q};
+	const iq_links L(q);
 	uint32_t got = 0, served = 0;
 	bool more = want;
 	for (uint32_t turn = 0; __any_sync(active, more) && turn < 33; turn++) {

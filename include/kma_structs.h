@@ -173,6 +173,8 @@ typedef struct kma_c3_queue_stats {
 	uint32_t err;            /* KMA_FLAG_TIMEOUT if a spin expired */
 	uint32_t walk_ok;        /* 1 when every shard's list ends at its tail with no cycle */
 	float enqueue_ms, dequeue_ms;
+	uint32_t log_chains;     /* warp forms: chains dequeued whole from their log records */
+	uint32_t pad;
 } kma_c3_queue_stats;
 
 /* Config-3 queue run: `threads` device threads each enqueue `per_thread`

@@ -66,7 +66,7 @@ class KmaC3QueueStats(Structure):
                 ("remaining", c_uint64), ("out_count", c_uint64), ("out_xor", c_uint64),
                 ("out_sum", c_uint64), ("in_xor", c_uint64), ("in_sum", c_uint64),
                 ("err", c_uint32), ("walk_ok", c_uint32), ("enqueue_ms", c_float),
-                ("dequeue_ms", c_float)]
+                ("dequeue_ms", c_float), ("log_chains", c_uint32), ("pad", c_uint32)]
 
 
 class KmaC3TreeStats(Structure):

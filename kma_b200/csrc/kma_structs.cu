@@ -1141,6 +1141,13 @@ extern "C" int kma_c3_queue_run(int kind, uint32_t threads, uint32_t per_thread,
 		st->err = e;
 		cudaEventElapsedTime(&st->enqueue_ms, e0, e1);
 		cudaEventElapsedTime(&st->dequeue_ms, e1, e2);
+		if (log) {
+			kma_chain_log hl;
+			unsigned int cnt[2] = {0, 0};
+			if (cudaMemcpy(&hl, log->dl, sizeof(hl), cudaMemcpyDeviceToHost) == cudaSuccess &&
+			    cudaMemcpy(cnt, hl.next, sizeof(cnt), cudaMemcpyDeviceToHost) == cudaSuccess)
+				st->log_chains = cnt[1];
+		}
 	}
 	if (iq)
 		kma_iqueue_destroy(iq);

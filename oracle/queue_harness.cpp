@@ -110,19 +110,18 @@ const uint32_t HOPS = 3;
 
 /* The chain log: records of 32 items, reused modulo the record count. */
 struct HostLog {
+	static constexpr bool enabled = true;
 	std::vector<u64> clq;
 	std::vector<uint32_t> iq;
 	uint32_t mask = 0;
 	std::atomic<uint32_t> next{0};
-	u64 clq_item(uint32_t recno, uint32_t j) const
-	{
-		return __atomic_load_n(&clq[(size_t)(recno & mask) * 32 + j], __ATOMIC_RELAXED);
-	}
-	uint32_t iq_item(uint32_t recno, uint32_t j) const
-	{
-		return __atomic_load_n(&iq[(size_t)(recno & mask) * 32 + j], __ATOMIC_RELAXED);
-	}
+	const u64 *clq_record(uint32_t recno) const { return &clq[(size_t)(recno & mask) * 32]; }
+	const uint32_t *iq_record(uint32_t recno) const { return &iq[(size_t)(recno & mask) * 32]; }
+	static u64 ld(const u64 *p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+	static uint32_t ld(const uint32_t *p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
 	uint32_t take() { return next.fetch_add(1) & kma_q::LOG_RECNO_MASK; }
+	mutable std::atomic<uint64_t> chains{0};
+	void taken(uint32_t) const { chains++; }
 };
 HostLog g_log;
 const HostLog *log_ptr() { return g_log.mask || !g_log.clq.empty() || !g_log.iq.empty() ? &g_log : nullptr; }
@@ -417,10 +416,10 @@ int main(int argc, char **argv)
 		run_iq(threads, chains, maxc, batch, recycle, seed, R);
 	double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 	const bool ok = R.bad == 0 && R.order == 0 && R.timeouts == 0;
-	printf("{\"queue\": \"%s\", \"log_records\": %u, \"threads\": %d, \"appended\": %llu, \"taken\": %llu, \"left\": %llu, "
+	printf("{\"queue\": \"%s\", \"log_records\": %u, \"log_chains\": %llu, \"threads\": %d, \"appended\": %llu, \"taken\": %llu, \"left\": %llu, "
 	       "\"conservation_faults\": %llu, \"order_faults\": %llu, \"timeouts\": %llu, \"delays\": %llu, "
 	       "\"seconds\": %.3f, \"ok\": %s}\n",
-	       clq ? "clq" : "iq", log_records, threads, (unsigned long long)R.enq, (unsigned long long)R.deq,
+	       clq ? "clq" : "iq", log_records, (unsigned long long)g_log.chains.load(), threads, (unsigned long long)R.enq, (unsigned long long)R.deq,
 	       (unsigned long long)R.left, (unsigned long long)R.bad, (unsigned long long)R.order,
 	       (unsigned long long)R.timeouts, (unsigned long long)g_delays.load(), s, ok ? "true" : "false");
 	return ok ? 0 : 1;
