@@ -233,7 +233,8 @@ def c3_line(kind: int, threads: int, per: int, shards: int) -> dict:
     ok = (st["out_count"] == n and st["out_xor"] == st["in_xor"] and st["out_sum"] == st["in_sum"]
           and st["walk_ok"] == 1 and st["err"] == 0)
     t = (st["enqueue_ms"] + st["dequeue_ms"]) / 1e3
-    return {"payloads": n, "threads": threads, "shards": shards, "warp_calls": bool(kind & structs.C3_WARP),
+    form = "block" if kind & structs.C3_BLOCK else ("warp" if kind & structs.C3_WARP else "thread")
+    return {"payloads": n, "threads": threads, "shards": shards, "calls": form,
             "conserved": bool(ok), "enqueue_mops": round(n / st["enqueue_ms"] / 1e3, 2),
             "dequeue_mops": round(n / st["dequeue_ms"] / 1e3, 2), "mops": round(2 * n / t / 1e6, 2)}
 
@@ -265,13 +266,15 @@ def measure_forms(quick: bool = False) -> dict:
     out = {}
     # config 3: one clQueue and one clIndexedQueue (the reference's single
     # structures), 2^24 payloads by 2^18 threads x 64, through the warp
-    # forms; the per-thread calls on one queue at 2^16 payloads (at full
-    # size their waits on the one head run out); 4096 independent shards
-    # as an extra
+    # forms and through the block forms (warp-chained enqueues, dequeues
+    # combined per block of 256); the per-thread calls on one queue at 2^16
+    # payloads (at full size their waits on the one head run out); 4096
+    # independent shards as an extra
     c3 = {}
     big = (1 << 18, 64) if not quick else (1 << 14, 64)
     for name, kind in (("clqueue", structs.C3_CLQUEUE), ("iqueue", structs.C3_IQUEUE)):
         c3[f"{name}_single"] = c3_line(kind | structs.C3_WARP, big[0], big[1], 1)
+        c3[f"{name}_single_block"] = c3_line(kind | structs.C3_BLOCK, big[0], big[1], 1)
         c3[f"{name}_single_per_thread_small"] = c3_line(kind, 1 << 12, 16, 1)
         c3[f"{name}_shards4096"] = c3_line(kind, big[0], big[1], 4096)
         c3[f"{name}_shards4096_warp"] = c3_line(kind | structs.C3_WARP, big[0], big[1], 4096)

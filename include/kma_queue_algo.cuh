@@ -261,9 +261,22 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 		 * links while the head is held (the items behind a held head
 		 * cannot move), gives the chain without walking it */
 		u64 nh = 0;
-		const uint32_t m = clq_chain_from_log<O, L>(log, hp, nx, out, k, &nh);
+		uint32_t m = clq_chain_from_log<O, L>(log, hp, nx, out, k, &nh);
 		if (m) {
 			log->taken(m);
+			/* more whole chains behind it, still under the same hold:
+			 * each costs its first link, its record number, its record
+			 * and its links, not a hold of its own */
+			while (m < k && nh != 0) {
+				u64 nh2 = 0;
+				const uint32_t m2 =
+					clq_chain_from_log<O, L>(log, nh, O::ld_rlx(L::at(nh)), out + m, k - m, &nh2);
+				if (!m2)
+					break;
+				log->taken(m2);
+				m += m2;
+				nh = nh2;
+			}
 			for (uint32_t j = 1; j < m; j++)
 				O::st_rlx(L::at(out[j]), POISON);
 			O::st(headw, qp_next(h, nh));
@@ -466,6 +479,18 @@ KQ_FN uint32_t iq_dequeue_n(const Q &q, u64 *headw, uint32_t *out, uint32_t k, u
 		if (r) {
 			log->taken(r);
 			cur = nh;
+			/* more whole chains behind it under the same hold (see
+			 * clq_dequeue_n); the head item's link is read with acquire,
+			 * as the first one */
+			while (r < k) {
+				uint32_t nh2 = 0;
+				const uint32_t r2 = iq_chain_from_log<O>(q, log, cur, O::ld(q.link(cur)), out + r, k - r, &nh2);
+				if (!r2)
+					break;
+				log->taken(r2);
+				r += r2;
+				cur = nh2;
+			}
 		} else {
 			while (r < k) {
 				const uint32_t nx = tw_idx(O::ld(q.link(cur)));

@@ -397,6 +397,71 @@ __device__ inline kma_clqueue_item *kma_clqueue_dequeue_warp(kma_clqueue *q, uin
 	return reinterpret_cast<kma_clqueue_item *>(got);
 }
 
+namespace kma_detail {
+/* Linear thread index of the block. */
+__device__ __forceinline__ uint32_t block_tid()
+{
+	return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+}
+/* Block-wide numbering of the threads with `want` set: every thread of the
+ * block calls it.  Returns this thread's number (warps in the order their
+ * leaders arrive, lanes in order within a warp) and the count in *total;
+ * *cnt is a shared word used as the counter. */
+__device__ inline uint32_t block_rank(bool want, unsigned int *cnt, uint32_t *total)
+{
+	if (block_tid() == 0)
+		*cnt = 0;
+	__syncthreads();
+	const uint32_t active = __activemask();
+	const uint32_t b = __ballot_sync(active, want);
+	const uint32_t leader = __ffs(active) - 1;
+	uint32_t base = 0;
+	if (lane_id() == leader && b)
+		base = atomicAdd(cnt, (unsigned int)__popc(b));
+	base = __shfl_sync(active, base, leader);
+	__syncthreads();
+	*total = *cnt;
+	return base + __popc(b & lanemask_lt());
+}
+} /* namespace kma_detail */
+
+/* Block form of dequeue: every thread of the block calls it, all with the
+ * same q; a thread with `want` false takes nothing (NULL).  One thread
+ * serves the block's requests, in turns of one hold of the head each, and
+ * a hold takes several logged chains in a row, so a block takes its items
+ * in a few more round trips than a warp takes its own instead of one hold
+ * per warp.  smem: blockDim + 1 words of shared memory the call may use.
+ * Items go to the wanting threads in the order block_rank numbers them;
+ * threads left over when the queue runs empty get NULL.  No counterpart in
+ * the reference. */
+__device__ inline kma_clqueue_item *kma_clqueue_dequeue_block(kma_clqueue *q, bool want, unsigned long long *smem,
+		uint32_t *err = nullptr, uint32_t spin_limit = KMA_STRUCT_SPIN, const kma_chain_log *log = nullptr)
+{
+	using namespace kma_detail;
+	unsigned int *w = reinterpret_cast<unsigned int *>(smem);
+	uint32_t k = 0;
+	const uint32_t rank = block_rank(want && q, &w[0], &k);
+	unsigned long long *out = smem + 1;
+	if (block_tid() == 0) {
+		uint32_t served = 0;
+		for (uint32_t turn = 0; q && served < k && turn < k; turn++) {
+			bool timed_out = false;
+			const uint32_t r = kma_q::clq_dequeue_n<gpu_ops, clq_link_head>(&q->head, &q->tail, out + served,
+											 k - served, spin_limit, &timed_out, log);
+			if (timed_out)
+				flag_err(err, KMA_ERR_TIMEOUT);
+			if (r == 0)
+				break;
+			served += r;
+		}
+		w[1] = served;
+	}
+	__syncthreads();
+	const unsigned long long got = want && q && rank < w[1] ? out[rank] : 0ull;
+	__syncthreads();
+	return reinterpret_cast<kma_clqueue_item *>(got);
+}
+
 /* The first item (NULL when empty), for walks from the head. */
 __device__ __forceinline__ kma_clqueue_item *kma_clqueue_first(const kma_clqueue *q)
 {
@@ -652,6 +717,52 @@ __device__ inline void *kma_iqueue_dequeue_warp_shard(kma_iqueue *q, uint32_t sh
 		}
 	}
 	return got ? kma_iqueue_item(q, got) : nullptr;
+}
+
+/* Block form of dequeue on one shard (see kma_clqueue_dequeue_block):
+ * every thread of the block calls it with the same q and shard; smem:
+ * blockDim + 1 words.  An internal dummy leaving the shard is skipped.
+ * No counterpart in the reference. */
+__device__ inline void *kma_iqueue_dequeue_block_shard(kma_iqueue *q, uint32_t shard, bool want,
+		unsigned long long *smem)
+{
+	using namespace kma_detail;
+	unsigned int *w = reinterpret_cast<unsigned int *>(smem);
+	uint32_t k = 0;
+	const uint32_t rank = block_rank(want, &w[0], &k);
+	uint32_t *out = reinterpret_cast<uint32_t *>(smem + 1);
+	if (block_tid() == 0) {
+		const iq_links L(q);
+		const uint32_t cap = L.capacity;
+		uint32_t served = 0;
+		for (uint32_t turn = 0; served < k && turn <= k; turn++) {
+			bool timed_out = false;
+			const uint32_t r = kma_q::iq_dequeue_n<gpu_ops>(L, &q->ends[2 * shard].v, out + served, k - served,
+									q->spin_limit, &timed_out,
+									(const kma_chain_log *)q->log);
+			if (timed_out)
+				atomicOr(&q->err, KMA_ERR_TIMEOUT);
+			if (r == 0)
+				break;
+			/* internal dummies leave silently */
+			uint32_t kept = 0;
+			for (uint32_t j = 0; j < r; j++)
+				if (out[served + j] <= cap)
+					out[served + kept++] = out[served + j];
+			served += kept;
+		}
+		w[1] = served;
+	}
+	__syncthreads();
+	const uint32_t got = want && rank < w[1] ? out[rank] : 0u;
+	__syncthreads();
+	return got ? kma_iqueue_item(q, got) : nullptr;
+}
+
+/* Block form on shard 0, the reference's queue. */
+__device__ __forceinline__ void *kma_iqueue_dequeue_block(kma_iqueue *q, bool want, unsigned long long *smem)
+{
+	return kma_iqueue_dequeue_block_shard(q, 0, want, smem);
 }
 
 __device__ __forceinline__ int kma_iqueue_enqueue_warp(kma_iqueue *q, void *item)

@@ -160,6 +160,11 @@ int kma_iqueue_set_chain_log(kma_iqueue_t q, kma_chain_log_t l, void *stream);
  * and its dequeues take consecutive items together; the queues get a
  * chain log of one record per 16 payloads (a power of two) */
 #define KMA_C3_WARP 0x100
+/* or'ed into the kind: enqueues through the warp forms, dequeues through
+ * the block forms (kma_clqueue_dequeue_block, kma_iqueue_dequeue_block):
+ * a block of 256 threads takes its items with one thread, several logged
+ * chains per hold of the head.  One queue only (shards must be 1). */
+#define KMA_C3_BLOCK 0x200
 
 typedef struct kma_c3_queue_stats {
 	uint64_t enqueued;       /* successful enqueues */

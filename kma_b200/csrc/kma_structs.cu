@@ -910,6 +910,33 @@ __global__ void k_c3_clq_deq(unsigned char *qs, uint32_t shards, uint32_t per_th
 		atomicAdd(&acc[6], e);
 }
 
+/* the block form on one queue: every thread of every block calls it */
+__global__ void __launch_bounds__(256) k_c3_clq_deq_block(kma_clqueue *q, uint32_t per_thread, uint32_t threads,
+		unsigned long long *acc, uint32_t *err, const kma_chain_log *log)
+{
+	__shared__ unsigned long long smem[256 + 1];
+	const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+	unsigned long long c = 0, x = 0, s = 0, e = 0;
+	for (uint32_t k = 0; k < per_thread; k++) {
+		kma_clqueue_item *it = kma_clqueue_dequeue_block(q, t < threads, smem, err, KMA_STRUCT_SPIN, log);
+		if (t >= threads)
+			continue;
+		if (!it) {
+			e++;
+			continue;
+		}
+		uint32_t pay = *(volatile uint32_t *)((unsigned char *)it + 8);
+		c++;
+		x ^= pay;
+		s += pay;
+	}
+	warp_flush(acc + 3, c, x, s);
+	for (int d = 16; d > 0; d >>= 1)
+		e += __shfl_down_sync(0xffffffffu, e, d);
+	if ((threadIdx.x & 31) == 0 && e)
+		atomicAdd(&acc[6], e);
+}
+
 /* one thread per shard: walk what is left; it counts as "out" too */
 __global__ void k_c3_clq_walk(unsigned char *qs, uint32_t shards, uint64_t n, unsigned long long *acc)
 {
@@ -1003,6 +1030,43 @@ __global__ void k_c3_iq_deq(kma_iqueue *q, uint32_t per_thread, uint32_t threads
 	}
 }
 
+/* the block form on shard 0 (one queue): every thread of every block calls it */
+__global__ void __launch_bounds__(256) k_c3_iq_deq_block(kma_iqueue *q, uint32_t per_thread, uint32_t threads,
+		unsigned long long *acc)
+{
+	__shared__ unsigned long long smem[256 + 1];
+	const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+	unsigned long long c = 0, x = 0, s = 0, e = 0, d0 = 0;
+	for (uint32_t k = 0; k < per_thread; k++) {
+		unsigned char *it = (unsigned char *)kma_iqueue_dequeue_block(q, t < threads, smem);
+		if (t >= threads)
+			continue;
+		if (!it) {
+			e++;
+			continue;
+		}
+		if (it == q->base) {
+			d0++; /* the initial dummy carries no payload */
+			continue;
+		}
+		uint32_t pay = *(volatile uint32_t *)(it + 8);
+		c++;
+		x ^= pay;
+		s += pay;
+	}
+	warp_flush(acc + 3, c, x, s);
+	for (int d = 16; d > 0; d >>= 1) {
+		e += __shfl_down_sync(0xffffffffu, e, d);
+		d0 += __shfl_down_sync(0xffffffffu, d0, d);
+	}
+	if ((threadIdx.x & 31) == 0) {
+		if (e)
+			atomicAdd(&acc[6], e);
+		if (d0)
+			atomicAdd(&acc[9], d0);
+	}
+}
+
 __global__ void k_c3_iq_walk(kma_iqueue *q, uint64_t n, unsigned long long *acc)
 {
 	uint32_t sh = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1038,10 +1102,11 @@ __global__ void k_c3_iq_walk(kma_iqueue *q, uint64_t n, unsigned long long *acc)
 extern "C" int kma_c3_queue_run(int kind, uint32_t threads, uint32_t per_thread, uint32_t shards, uint64_t seed,
 		int device, kma_c3_queue_stats *st)
 {
-	const bool warp = kind & KMA_C3_WARP;
-	kind &= ~KMA_C3_WARP;
+	const bool block = kind & KMA_C3_BLOCK;
+	const bool warp = (kind & KMA_C3_WARP) || block;
+	kind &= ~(KMA_C3_WARP | KMA_C3_BLOCK);
 	if (!st || threads == 0 || per_thread == 0 || shards == 0 || shards > KMA_IQ_MAX_SHARDS ||
-	    (kind != KMA_C3_CLQUEUE && kind != KMA_C3_IQUEUE))
+	    (kind != KMA_C3_CLQUEUE && kind != KMA_C3_IQUEUE) || (block && shards != 1))
 		return KMA_EINVAL;
 	uint64_t n64 = (uint64_t)threads * per_thread;
 	if (n64 >= 0x7fffffffull)
@@ -1091,7 +1156,9 @@ extern "C" int kma_c3_queue_run(int kind, uint32_t threads, uint32_t per_thread,
 			else
 				k_c3_clq_enq<false><<<blocks, 256>>>(qs, shards, items, per_thread, n, seed, acc, err, dl);
 			cudaEventRecord(e1);
-			if (warp)
+			if (block)
+				k_c3_clq_deq_block<<<blocks, 256>>>((kma_clqueue *)qs, per_thread, threads, acc, err, dl);
+			else if (warp)
 				k_c3_clq_deq<true><<<blocks, 256>>>(qs, shards, per_thread, threads, acc, err, dl);
 			else
 				k_c3_clq_deq<false><<<blocks, 256>>>(qs, shards, per_thread, threads, acc, err, dl);
@@ -1109,7 +1176,9 @@ extern "C" int kma_c3_queue_run(int kind, uint32_t threads, uint32_t per_thread,
 			else
 				k_c3_iq_enq<false><<<blocks, 256>>>(iq->dq, per_thread, n, seed, acc);
 			cudaEventRecord(e1);
-			if (warp)
+			if (block)
+				k_c3_iq_deq_block<<<blocks, 256>>>(iq->dq, per_thread, threads, acc);
+			else if (warp)
 				k_c3_iq_deq<true><<<blocks, 256>>>(iq->dq, per_thread, threads, acc);
 			else
 				k_c3_iq_deq<false><<<blocks, 256>>>(iq->dq, per_thread, threads, acc);

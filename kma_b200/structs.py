@@ -21,6 +21,7 @@ from .heap import Heap, _stream_ptr
 C3_CLQUEUE = 0
 C3_IQUEUE = 1
 C3_WARP = 0x100  # or into the kind: warp-combined enqueues and dequeues
+C3_BLOCK = 0x200  # or into the kind: warp-combined enqueues, block-combined dequeues (one queue)
 
 
 class _Handle:

@@ -36,6 +36,7 @@
  * (serial replays against tests/golden); this program checks this build's
  * concurrent behaviour.
  */
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cstdio>
@@ -234,7 +235,10 @@ void run_clq(int threads, int chains, int maxc, int batch, double recycle, uint6
 			}
 			bk.deq += r;
 			if (!back.empty())
-				append(back.data(), (int)back.size(), (uint32_t)(np + c), seq);
+				/* re-appended in chains of at most 32, a warp's */
+				for (size_t o = 0; o < back.size(); o += 32)
+					append(back.data() + o, (int)std::min<size_t>(32, back.size() - o), (uint32_t)(np + c),
+					       seq);
 			if (to || bk.runaway())
 				break;
 			if (r == 0 && done && kma_q::qp_ptr(HostOps::ld(&q[0])) == 0)
@@ -348,7 +352,10 @@ void run_iq(int threads, int chains, int maxc, int batch, double recycle, uint64
 			}
 			bk.deq += r;
 			if (!back.empty())
-				append(back.data(), (int)back.size(), (uint32_t)(np + c), seq);
+				/* re-appended in chains of at most 32, a warp's */
+				for (size_t o = 0; o < back.size(); o += 32)
+					append(back.data() + o, (int)std::min<size_t>(32, back.size() - o), (uint32_t)(np + c),
+					       seq);
 			if ((r == 0 && done) || to || bk.runaway())
 				break;
 		}

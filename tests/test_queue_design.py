@@ -39,6 +39,12 @@ CONFIGS = [
     "8 5000 32 32 0.02 8 4 0.5 8",
     "8 20000 8 8 0.01 9 2 0.5 2",
     "8 40000 32 32 0.0005 10 4 0 1024",
+    # batches larger than a chain: one hold takes several logged chains
+    # (the block forms), with long and short chains, large and stale logs
+    "8 5000 32 128 0.02 11 4 0.5 65536",
+    "8 5000 32 256 0.02 12 4 0.5 8",
+    "8 20000 8 64 0.01 13 2 0.5 1024",
+    "8 40000 32 256 0.0005 14 4 0 1024",
 ]
 
 
@@ -87,6 +93,14 @@ MUTANTS = {
                               "\t\tif (true) { O::st(tailw, 0ull);"),
     # take the indexed queue's head hold with a plain store: two dequeuers
     # hold it at once and take the same items
+    # a hold that takes several chains forgets to return the later ones
+    # (shows that batches larger than a chain do take several chains)
+    "multi_chain_dropped": ("clq", "8 5000 32 128 0.02 11 4 0.5 65536",
+                            "\t\t\t\tm += m2;\n",
+                            "\t\t\t\t(void)m2;\n"),
+    "iq_multi_chain_dropped": ("iq", "8 5000 32 128 0.02 11 4 0.5 65536",
+                               "\t\t\t\tr += r2;\n",
+                               "\t\t\t\t(void)r2;\n"),
     "iq_hold_store": ("iq", "8 20000 4 4 0.01 2 2 0.5",
                       "\t\tif (O::cas(headw, hd, tw_make(tw_tag(hd) + 1u, cur)) != hd) {",
                       "\t\tO::st(headw, tw_make(tw_tag(hd) + 1u, cur));\n\t\tif (false) {"),

@@ -247,21 +247,28 @@ def test_gpu_arraylist_on_pma_is_a_bump_sequence():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind", [0, 1], ids=["clqueue", "iqueue"])
-@pytest.mark.parametrize("shards", [1, 64])
-def test_gpu_c3_queue_conserves_payloads(kind, shards):
+@pytest.mark.parametrize("form,shards,threads,per", [
+    ("thread", 1, 4096, 16), ("thread", 64, 4096, 16),
+    ("warp", 1, 4096, 16), ("warp", 64, 4096, 16), ("warp", 1, 1000, 7),
+    ("block", 1, 4096, 16), ("block", 1, 1000, 7), ("block", 1, 1 << 16, 64),
+])
+def test_gpu_c3_queue_conserves_payloads(kind, form, shards, threads, per):
+    """Every payload enqueued is dequeued once (per-thread calls, the warp
+    forms with their chain log, and the block forms, whose holds take
+    several chains), and the queue's links end consistent with its tail;
+    thread counts that leave partial warps and blocks included."""
     from kma_b200 import structs
-    threads, per = 4096, 16
-    st = structs.c3_queue(kind, threads, per, shards, seed=0xC3)
+    flag = {"thread": 0, "warp": structs.C3_WARP, "block": structs.C3_BLOCK}[form]
+    st = structs.c3_queue(kind | flag, threads, per, shards, seed=0xC3)
+    if form != "thread" and shards == 1:
+        assert st["log_chains"] > 0  # (over 64 shards a warp's lanes name different queues: no chains)
     n = threads * per
     assert st["err"] == 0 and st["walk_ok"] == 1
     assert st["enqueued"] == n
     assert st["out_count"] == n
     assert st["out_xor"] == st["in_xor"] and st["out_sum"] == st["in_sum"]
     assert st["in_sum"] == n * (n - 1) // 2  # the payloads are a permutation of 0..n-1
-    x = 0
-    for v in range(n):
-        x ^= v
-    assert st["in_xor"] == x
+    assert st["in_xor"] == int(np.bitwise_xor.reduce(np.arange(n, dtype=np.uint64)))
 
 
 @pytest.mark.gpu
