@@ -49,8 +49,10 @@
  *   ld_rlx(p)    relaxed load        st_rlx(p, v) relaxed store
  *   xchg(p, v)   acq_rel exchange    cas(p, c, v) acq_rel compare-and-swap, returns the old value
  *   pause(it)    back-off after `it` fruitless tries
- * Every wait is bounded by `limit` tries; expiry returns failure and the
- * caller records KMA_ERR_TIMEOUT.
+ * Every wait is bounded by `limit` tries (a dequeue's: tries in which the
+ * queue's head did not move, so a waiter is not failed while others make
+ * progress; a head that stops moving ends every wait); expiry returns
+ * failure and the caller records KMA_ERR_TIMEOUT.
  */
 #ifndef KMA_QUEUE_ALGO_CUH
 #define KMA_QUEUE_ALGO_CUH
@@ -226,13 +228,23 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 		const LG *log)
 {
 	*timed_out = false;
-	uint32_t it = 0;
-	while (it < limit) {
+	uint32_t it = 0, idle = 0;
+	u64 last = ~0ull;
+	for (;;) {
 		/* waiters poll with relaxed loads: an acquire load also invalidates
 		 * the SM's L1 on the GPU (under contention thousands of waiters
 		 * would keep evicting the holder's local data); the exchange that
 		 * takes the head item is the acquire */
 		const u64 h = O::ld_rlx(headw);
+		/* `limit` bounds the tries in which the head did not move: one of
+		 * many waiters on a head may wait long while the others take
+		 * items, and only a head that stops moving means a stuck queue */
+		if (h != last) {
+			last = h;
+			idle = 0;
+		} else if (++idle >= limit) {
+			break;
+		}
 		const u64 hp = qp_ptr(h);
 		if (hp == 0)
 			return 0;
@@ -307,8 +319,10 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 		}
 		/* give the link back and wait for the append to land */
 		O::st(hl, 0ull);
-		while (it < limit && O::ld(hl) == 0ull && O::ld(headw) == h)
+		while (idle < limit && O::ld(hl) == 0ull && O::ld(headw) == h) {
 			O::pause(it++);
+			idle++;
+		}
 	}
 	*timed_out = true;
 	return 0;
@@ -451,10 +465,19 @@ KQ_FN uint32_t iq_dequeue_n(const Q &q, u64 *headw, uint32_t *out, uint32_t k, u
 		const LG *log)
 {
 	*timed_out = false;
-	for (uint32_t it = 0; it < limit; it++) {
+	uint32_t idle = 0;
+	u64 last = ~0ull;
+	for (uint32_t it = 0;; it++) {
 		/* relaxed polling, as in clq_dequeue_n; the CAS that takes the
-		 * head is the acquire */
+		 * head is the acquire.  `limit` bounds the tries in which the
+		 * head did not move (see clq_dequeue_n). */
 		const u64 hd = O::ld_rlx(headw);
+		if (hd != last) {
+			last = hd;
+			idle = 0;
+		} else if (++idle >= limit) {
+			break;
+		}
 		if (iq_head_held(hd)) {
 			O::pause(it);
 			continue;

@@ -26,7 +26,7 @@
 
 #define KMA_STRUCT_SPIN (1u << 20)
 #ifndef KMA_QUEUE_PAUSE_MAX_NS
-#define KMA_QUEUE_PAUSE_MAX_NS 4096u
+#define KMA_QUEUE_PAUSE_MAX_NS 512u
 #endif
 
 namespace kma_detail {

@@ -391,11 +391,59 @@ void run_iq(int threads, int chains, int maxc, int batch, double recycle, uint64
 
 } /* namespace */
 
+/* Stuck queues (a dequeuer that died holding the head, an append that
+ * exchanged the tail and never linked): every wait must end, within
+ * `limit` tries in which the head did not move, and report the expiry. */
+int run_stuck()
+{
+	const uint32_t limit = 1000;
+	bool ok = true;
+	{
+		Item a{}, b{};
+		u64 q[2] = {(u64)&a, (u64)&b};
+		a.next = kma_q::POISON; /* held by a dequeuer that is gone */
+		b.next = 0;
+		(void)b;
+		u64 out[4];
+		bool to = false;
+		uint32_t r = kma_q::clq_dequeue_n<HostOps, LinkAtItem>(&q[0], &q[1], out, 4, limit, &to,
+								      (const HostLog *)nullptr);
+		printf("{\"case\": \"clq_head_held\", \"taken\": %u, \"timed_out\": %s}\n", r, to ? "true" : "false");
+		ok &= r == 0 && to && a.next == kma_q::POISON;
+	}
+	{
+		Item a{}, b{};
+		u64 q[2] = {(u64)&a, (u64)&b}; /* b's append exchanged the tail, never linked */
+		a.next = 0;
+		u64 out[4];
+		bool to = false;
+		uint32_t r = kma_q::clq_dequeue_n<HostOps, LinkAtItem>(&q[0], &q[1], out, 4, limit, &to,
+								      (const HostLog *)nullptr);
+		printf("{\"case\": \"clq_append_unlinked\", \"taken\": %u, \"timed_out\": %s}\n", r, to ? "true" : "false");
+		ok &= r == 0 && to && a.next == 0 && q[0] == (u64)&a;
+	}
+	{
+		std::vector<u64> links(4, 0);
+		IdxQ iq{&links};
+		links[1] = kma_q::tw_make(0, 2); /* dummy 1 -> item 2 */
+		u64 ends[2] = {kma_q::tw_make(1, 1), kma_q::tw_make(0, 2)}; /* head held (odd tag) */
+		uint32_t out[4];
+		bool to = false;
+		uint32_t r = kma_q::iq_dequeue_n<HostOps>(iq, &ends[0], out, 4, limit, &to, (const HostLog *)nullptr);
+		printf("{\"case\": \"iq_head_held\", \"taken\": %u, \"timed_out\": %s}\n", r, to ? "true" : "false");
+		ok &= r == 0 && to && ends[0] == kma_q::tw_make(1, 1);
+	}
+	printf("{\"stuck_ok\": %s}\n", ok ? "true" : "false");
+	return ok ? 0 : 1;
+}
+
 int main(int argc, char **argv)
 {
+	if (argc == 2 && strcmp(argv[1], "stuck") == 0)
+		return run_stuck();
 	if (argc < 8 || argc > 11) {
 		fprintf(stderr, "usage: %s clq|iq THREADS CHAINS MAX_CHAIN DEQ_BATCH DELAY_PROB SEED "
-			"[PRODUCERS [RECYCLE [LOG_RECORDS]]]\n", argv[0]);
+			"[PRODUCERS [RECYCLE [LOG_RECORDS]]]\n       %s stuck\n", argv[0], argv[0]);
 		return 2;
 	}
 	const bool clq = strcmp(argv[1], "clq") == 0;

@@ -75,6 +75,18 @@ def test_queue_algorithm_conserves_and_keeps_order(harness, kind, cfg):
     assert st["conservation_faults"] == 0 and st["order_faults"] == 0 and st["timeouts"] == 0
 
 
+def test_stuck_queues_end_every_wait(harness):
+    """A dequeuer that died holding the head, and an append that exchanged
+    the tail but never linked: a dequeue on such a queue gives up after
+    `limit` tries in which the head did not move, reports the expiry and
+    leaves the queue as it found it."""
+    r = subprocess.run([harness, "stuck"], capture_output=True, text=True, timeout=60)
+    lines = [json.loads(x) for x in r.stdout.strip().splitlines()]
+    assert r.returncode == 0 and lines[-1] == {"stuck_ok": True}, r.stdout
+    assert {x["case"] for x in lines[:-1]} == {"clq_head_held", "clq_append_unlinked", "iq_head_held"}
+    assert all(x["timed_out"] and x["taken"] == 0 for x in lines[:-1])
+
+
 # Each mutant breaks one step the algorithm depends on.
 MUTANTS = {
     # link after the previous tail with a plain store: a dequeuer's hold
