@@ -109,6 +109,19 @@ int kma_clqueue_replay_host(uint32_t n_items, const int64_t *ops, int64_t n, int
 int kma_iqueue_replay_host(uint32_t n_items, uint32_t stride_l2, const int64_t *ops, int64_t n,
 			   int64_t *out, int64_t *final_state);
 
+/* ---- fault injection (tests) ------------------------------------------ */
+/* No counterpart in the reference.  Builds a stuck queue on the device and
+ * runs one dequeue on it with the given spin limit: kind KMA_C3_CLQUEUE
+ * with state 0 (the head item's link left POISON by a dequeuer that is
+ * gone) or 1 (an append that exchanged the tail and never linked), kind
+ * KMA_C3_IQUEUE with state 0 (the head's hold tag left odd).  Nothing ever
+ * frees the queue, so the dequeue gives up after spin_limit tries in which
+ * the head did not move: *taken = -1 (NULL), *flags = the error flags it
+ * raised (KMA_FLAG_TIMEOUT), no device fault.  KMA_EINVAL for other
+ * kinds / states. */
+int kma_debug_queue_stuck_dequeue(int kind, int state, uint32_t spin_limit, int device, int64_t *taken,
+				  uint32_t *flags);
+
 /* ---- clTree ---------------------------------------------------------- */
 /* One-thread replay of a clTree (clTree.cl:27-74) with one 24-byte node per
  * op that the call allocates: ops (0, key) add -> 1 inserted, 0 exists,

@@ -427,6 +427,81 @@ __global__ void k_iq_replay(kma_iqueue *q, const int64_t *ops, int64_t n, int64_
 }
 } /* namespace */
 
+namespace {
+/* one thread: plant a stuck state, then one dequeue with spin limit `limit` */
+__global__ void k_dbg_stuck_clq(int state, uint32_t limit, unsigned long long *items, kma_clqueue *q, int64_t *out,
+				uint32_t *err)
+{
+	if (blockIdx.x != 0 || threadIdx.x != 0)
+		return;
+	unsigned long long a = (unsigned long long)&items[0], b = (unsigned long long)&items[2];
+	items[0] = state == 0 ? KMA_Q_POISON : 0ull; /* a's link */
+	items[2] = 0ull;                               /* b's link */
+	q->head = a;
+	q->tail = b; /* state 1: b's append exchanged the tail and stopped */
+	__threadfence();
+	*out = kma_detail::clq_dequeue<kma_detail::clq_link_head>(q, err, limit) ? 1 : -1;
+}
+__global__ void k_dbg_stuck_iq(uint32_t limit, kma_iqueue *q, int64_t *out)
+{
+	if (blockIdx.x != 0 || threadIdx.x != 0)
+		return;
+	q->spin_limit = limit;
+	const kma_detail::iq_links L(q);
+	kma_q::iq_set_link<kma_detail::gpu_ops>(L, 1u, 2u); /* dummy 1 -> item 2 */
+	q->ends[0].v = kma_q::tw_make(1u, 1u);              /* hold tag odd: held by nobody */
+	__threadfence();
+	void *it = kma_iqueue_dequeue_shard(q, 0);
+	*out = it ? 1 : -1;
+}
+} /* namespace */
+
+extern "C" int kma_debug_queue_stuck_dequeue(int kind, int state, uint32_t spin_limit, int device, int64_t *taken,
+		uint32_t *flags)
+{
+	if (!taken || !flags || spin_limit == 0 || !((kind == KMA_C3_CLQUEUE && (state == 0 || state == 1)) ||
+						    (kind == KMA_C3_IQUEUE && state == 0)))
+		return KMA_EINVAL;
+	kma_device_guard g(device);
+	if (!g.ok)
+		return KMA_ENODEV;
+	dev_bufs b;
+	int64_t *out = b.alloc<int64_t>(8);
+	uint32_t *err = b.alloc<uint32_t>(4);
+	unsigned long long *items = b.alloc<unsigned long long>(64); /* 4 items of 16 bytes */
+	if (!out || !err || !items)
+		return KMA_ENOMEM;
+	KMA_CUDA(cudaMemset(err, 0, 4));
+	KMA_CUDA(cudaMemset(items, 0, 64));
+	uint32_t e = 0;
+	if (kind == KMA_C3_CLQUEUE) {
+		kma_clqueue *q = b.alloc<kma_clqueue>(sizeof(kma_clqueue));
+		if (!q)
+			return KMA_ENOMEM;
+		k_dbg_stuck_clq<<<1, 1>>>(state, spin_limit, items, q, out, err);
+		KMA_CUDA(cudaGetLastError());
+		KMA_CUDA(cudaDeviceSynchronize());
+		KMA_CUDA(cudaMemcpy(&e, err, 4, cudaMemcpyDeviceToHost));
+	} else {
+		kma_iqueue_t q = NULL;
+		int rc = kma_iqueue_create(items, 4, 3, items, 1, -1, NULL, &q);
+		if (rc != KMA_OK)
+			return rc;
+		k_dbg_stuck_iq<<<1, 1>>>(spin_limit, q->dq, out);
+		if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+			kma_iqueue_destroy(q);
+			return KMA_ECUDA;
+		}
+		rc = kma_iqueue_error_flags(q, NULL, &e, 0);
+		kma_iqueue_destroy(q);
+		if (rc != KMA_OK)
+			return rc;
+	}
+	KMA_CUDA(cudaMemcpy(taken, out, 8, cudaMemcpyDeviceToHost));
+	*flags = e;
+	return KMA_OK;
+}
+
 extern "C" int kma_iqueue_replay_host(uint32_t n_items, uint32_t stride_l2, const int64_t *ops, int64_t n,
 		int64_t *out, int64_t *final_state)
 {

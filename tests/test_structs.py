@@ -272,6 +272,23 @@ def test_gpu_c3_queue_conserves_payloads(kind, form, shards, threads, per):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kind,state", [(0, 0), (0, 1), (1, 0)],
+                         ids=["clqueue_head_held", "clqueue_append_unlinked", "iqueue_head_held"])
+def test_gpu_stuck_queue_dequeue_gives_up_and_flags(kind, state):
+    """On the device, a dequeue on a queue nothing will ever free (a holder
+    that is gone, an append that never linked) ends after its spin limit,
+    returns NULL and raises the timeout flag: no hang, no fault."""
+    import ctypes
+    from kma_b200 import KMA_FLAG_TIMEOUT
+    from kma_b200._lib import lib
+    taken, flags = ctypes.c_int64(0), ctypes.c_uint32(0)
+    assert lib().kma_debug_queue_stuck_dequeue(kind, state, 4096, -1, ctypes.byref(taken),
+                                               ctypes.byref(flags)) == 0
+    assert taken.value == -1
+    assert flags.value & KMA_FLAG_TIMEOUT
+
+
+@pytest.mark.gpu
 def test_gpu_c3_tree_equals_sequential_replay():
     from kma_b200 import structs
     rng = np.random.default_rng(0xC3)
