@@ -210,7 +210,7 @@ __device__ __forceinline__ void bt_round(typename B::heap *h, const bt_dev &w, c
 			q = bt_block<B>(h, w.off4[e]);
 			qn = bt_bytes(w.meta[e]);
 		}
-		if (coop_verify_blockwise(mask, lane, q, qn, (uint32_t)o_g))
+		if (coop_verify(mask, lane, q, qn, (uint32_t)o_g))
 			ct.bad++;
 		bt_free<B, WARP>(h, cc, lane, q, qn, ct);
 		if (q) {
@@ -244,7 +244,7 @@ __device__ __forceinline__ void bt_round(typename B::heap *h, const bt_dev &w, c
 			q = bt_block<B>(h, w.off4[g]);
 			qn = bt_bytes(w.meta[g]);
 		}
-		if (coop_verify_blockwise(mask, lane, q, qn, tag))
+		if (coop_verify(mask, lane, q, qn, tag))
 			ct.bad++;
 		bt_free<B, WARP>(h, cc, lane, q, qn, ct);
 		if (full) {

@@ -209,8 +209,9 @@ __device__ __forceinline__ bool coop_verify_rows(uint32_t mask, uint32_t lane, c
  * reads its own with 16-byte loads unrolled by eight.  Blocks of
  * WL_COOP_BYTES or more: the calling lanes read each together, block by
  * block (each block's loads are consumed before the next block's are
- * issued, which suits kernels short of registers: the batched form's
- * measured faster so). */
+ * issued).  coop_verify's fallback when WL_VERIFY_SLOTS is 0; with the
+ * streaming payload hints the row batches measured faster in both the
+ * config-2 rounds kernel and the batched form (3737 vs 3633 M ops/s). */
 __device__ __forceinline__ bool coop_verify_blockwise(uint32_t mask, uint32_t lane, const void *p, uint32_t n,
 		uint32_t tag)
 {
