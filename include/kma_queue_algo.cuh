@@ -82,8 +82,8 @@ const u64 POISON = 1ull;
 const int PTR_BITS = 48;
 const u64 PTR_MASK = (1ull << PTR_BITS) - 1ull;
 
-/* chain log records: numbers of 25 bits, chains of at most 32 items */
-const uint32_t LOG_RECNO_MASK = 0x1FFFFFFu;
+/* chain log records: numbers of 24 bits, chains of at most 32 items */
+const uint32_t LOG_RECNO_MASK = 0xFFFFFFu;
 const uint32_t LOG_CHAIN_MAX = 32;
 
 /* The log policy of callers without a log: the log code compiles away. */
@@ -101,22 +101,33 @@ KQ_FN u64 qp_next(u64 w, u64 ptr) { return (((w >> PTR_BITS) + 1ull) << PTR_BITS
 
 /* A logged chain (at least 3 items) marks the top 16 bits of its first
  * two links: first = CLQ_LOG | (length - 1) << 10 | record number bits
- * 15..24, second = record number bits 0..14 (its top bit stays clear, so
- * it never reads as a first mark).  Every other link has them clear;
- * readers take the pointer with qp_ptr. */
+ * 14..23, second = record number bits 0..13 (its top two bits stay clear,
+ * so it never reads as a first or into mark).  The append that links the
+ * chain after the previous tail item marks that link too (the link INTO
+ * the chain): CLQ_INTO | record number bits 0..13, so that a dequeuer that
+ * reaches the chain over that link has its whole record number without
+ * loading the second link first.  Every other link has the top bits
+ * clear; readers take the pointer with qp_ptr. */
 const u64 CLQ_LOG = 0x8000ull << PTR_BITS;
+const u64 CLQ_INTO = 0x4000ull << PTR_BITS;
 KQ_FN u64 clq_mark_first(uint32_t recno, uint32_t len)
 {
-	return CLQ_LOG | ((u64)(((len - 1u) << 10) | ((recno >> 15) & 0x3FFu)) << PTR_BITS);
+	return CLQ_LOG | ((u64)(((len - 1u) << 10) | ((recno >> 14) & 0x3FFu)) << PTR_BITS);
 }
-KQ_FN u64 clq_mark_second(uint32_t recno) { return (u64)(recno & 0x7FFFu) << PTR_BITS; }
+KQ_FN u64 clq_mark_second(uint32_t recno) { return (u64)(recno & 0x3FFFu) << PTR_BITS; }
+KQ_FN u64 clq_mark_into(uint32_t recno) { return CLQ_INTO | ((u64)(recno & 0x3FFFu) << PTR_BITS); }
 
 /* Up to k items [hp, ...] of the logged chain that starts at hp (its link
  * v), if its record matches the links: fills out[], sets *nh to the item
- * after them, returns how many (0: no usable record).  Reads only. */
+ * after them, returns how many (0: no usable record).  `into`: the link
+ * that leads to hp as read (0 if unknown); *nh_link: the link that leads
+ * to *nh when the whole chain was taken, else 0.  Reads only. */
 template <class O, class L, class LG>
-KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32_t k, u64 *nh)
+KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32_t k, u64 *nh, u64 into = 0,
+		u64 *nh_link = nullptr)
 {
+	if (nh_link)
+		*nh_link = 0;
 	if constexpr (!LG::enabled)
 		return 0;
 	if (!log || !(v & CLQ_LOG) || k == 0)
@@ -129,15 +140,22 @@ KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32
 	/* relaxed loads, issued back to back into registers: an acquire load,
 	 * or a store of each value before the next load, would make them one
 	 * round trip each, as a walk.  The exchange that took the head
-	 * already ordered the chain's contents before these reads. */
-	const u64 l1 = O::ld_rlx(L::at(second));
-	const uint32_t recno = ((mark & 0x3FFu) << 15) | ((uint32_t)(l1 >> PTR_BITS) & 0x7FFFu);
+	 * already ordered the chain's contents before these reads.  The low
+	 * record-number bits come from the link into hp when it carries them
+	 * (then the second link loads with the others), else from the second
+	 * link, loaded first. */
+	const bool via_into = (into & CLQ_INTO) && !(into & CLQ_LOG) && qp_ptr(into) == hp;
+	u64 l1 = via_into ? 0ull : O::ld_rlx(L::at(second));
+	const uint32_t recno = ((mark & 0x3FFu) << 14) |
+			       ((uint32_t)((via_into ? into : l1) >> PTR_BITS) & 0x3FFFu);
 	uint32_t m = len < k ? len : k;
 	const u64 *rec = log->clq_record(recno);
 	u64 item[LOG_CHAIN_MAX];
 #pragma unroll
 	for (uint32_t j = 0; j < LOG_CHAIN_MAX; j++)
 		item[j] = j <= m && j < len ? LG::ld(rec + j) : 0ull;
+	if (via_into)
+		l1 = O::ld_rlx(L::at(second));
 	const u64 after = m < len ? item[m < LOG_CHAIN_MAX ? m : 0] : 0ull;
 	if (item[0] != hp || (m > 1 && item[1] != second) || (m > 2 && item[2] != qp_ptr(l1)))
 		return 0;
@@ -174,6 +192,8 @@ KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32
 		/* the chain's last item has no successor yet: it stays, as the head */
 		next = item[(m - 1) & (LOG_CHAIN_MAX - 1)];
 		m--;
+	} else if (nh_link) {
+		*nh_link = last;
 	}
 #pragma unroll
 	for (uint32_t j = 0; j < LOG_CHAIN_MAX; j++)
@@ -184,9 +204,11 @@ KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32
 }
 
 /* Append the chain first..last (its links already set, last's link 0,
- * all of it written before the call).  1, or 0 when a wait expired. */
+ * all of it written before the call).  `into`: mark bits for the link from
+ * the previous tail item to `first` (clq_mark_into of a logged chain, or
+ * 0).  1, or 0 when a wait expired. */
 template <class O, class L>
-KQ_FN int clq_append(u64 *headw, u64 *tailw, u64 first, u64 last, uint32_t limit)
+KQ_FN int clq_append(u64 *headw, u64 *tailw, u64 first, u64 last, uint32_t limit, u64 into = 0)
 {
 	const u64 prev = O::xchg(tailw, last);
 	if (prev == 0) {
@@ -204,7 +226,7 @@ KQ_FN int clq_append(u64 *headw, u64 *tailw, u64 first, u64 last, uint32_t limit
 	 * whether prev is the last item gives it back at once */
 	u64 *pl = L::at(prev);
 	for (uint32_t it = 0; it < limit; it++) {
-		const u64 old = O::cas(pl, 0ull, first);
+		const u64 old = O::cas(pl, 0ull, first | into);
 		if (old == 0)
 			return 1;
 		if (old != POISON)
@@ -272,22 +294,24 @@ KQ_FN uint32_t clq_dequeue_n(u64 *headw, u64 *tailw, u64 *out, uint32_t k, uint3
 		/* a logged chain at the head: its record, checked against the
 		 * links while the head is held (the items behind a held head
 		 * cannot move), gives the chain without walking it */
-		u64 nh = 0;
-		uint32_t m = clq_chain_from_log<O, L>(log, hp, nx, out, k, &nh);
+		u64 nh = 0, into = 0;
+		uint32_t m = clq_chain_from_log<O, L>(log, hp, nx, out, k, &nh, 0ull, &into);
 		if (m) {
 			log->taken(m);
 			/* more whole chains behind it, still under the same hold:
-			 * each costs its first link, its record number, its record
-			 * and its links, not a hold of its own */
+			 * each costs its first link, its record and its links (the
+			 * link that led to it carries the rest of its record
+			 * number), not a hold of its own */
 			while (m < k && nh != 0) {
-				u64 nh2 = 0;
-				const uint32_t m2 =
-					clq_chain_from_log<O, L>(log, nh, O::ld_rlx(L::at(nh)), out + m, k - m, &nh2);
+				u64 nh2 = 0, into2 = 0;
+				const uint32_t m2 = clq_chain_from_log<O, L>(log, nh, O::ld_rlx(L::at(nh)), out + m, k - m,
+									     &nh2, into, &into2);
 				if (!m2)
 					break;
 				log->taken(m2);
 				m += m2;
 				nh = nh2;
+				into = into2;
 			}
 			for (uint32_t j = 1; j < m; j++)
 				O::st_rlx(L::at(out[j]), POISON);
@@ -345,7 +369,7 @@ KQ_FN uint32_t tw_tag(u64 w) { return (uint32_t)(w >> 32); }
 KQ_FN u64 tw_make(uint32_t tag, uint32_t idx) { return ((u64)tag << 32) | idx; }
 
 /* Links need no ABA tag (nothing CASes them): a link's tag is 0, or, on
- * the first link of a logged chain, IQ_LOG | record number (25 bits) << 5 |
+ * the first link of a logged chain, IQ_LOG | record number (24 bits) << 5 |
  * (chain length - 1).  Head keeps a counting tag. */
 const uint32_t IQ_LOG = 0x80000000u;
 KQ_FN uint32_t iq_log_tag(uint32_t recno, uint32_t len)

@@ -360,7 +360,8 @@ __device__ inline int kma_clqueue_enqueue_warp(kma_clqueue *q, kma_clqueue_item 
 	__syncwarp(active);
 	int r = 0;
 	if (ok && lane == gp.first) {
-		r = kma_q::clq_append<gpu_ops_group, clq_link_head>(&q->head, &q->tail, ip, lip, spin_limit);
+		r = kma_q::clq_append<gpu_ops_group, clq_link_head>(&q->head, &q->tail, ip, lip, spin_limit,
+								       logged ? kma_q::clq_mark_into(recno) : 0ull);
 		if (!r)
 			flag_err(err, KMA_ERR_TIMEOUT);
 	}

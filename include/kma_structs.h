@@ -148,7 +148,7 @@ int kma_clarraylist_group_host(kma_heap_t kma, kma_pma_t pma, uint32_t obj_size,
 			       const uint32_t *objs, uint32_t n, int mode, int64_t *out);
 
 /* ---- chain log (kma_structs.cuh) ----------------------------------------- */
-/* A log of `records` (a power of two, at most 2^25) chain records for the
+/* A log of `records` (a power of two, at most 2^24) chain records for the
  * warp forms of the queues: warp enqueues record each chain's items, warp
  * dequeues take a recorded chain at the head in one step instead of
  * walking it.  256 bytes per record; records are reused round robin and

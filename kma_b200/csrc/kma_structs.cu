@@ -539,7 +539,7 @@ extern "C" int kma_chain_log_create(uint32_t records, int device, void *stream, 
 	if (!out)
 		return KMA_EINVAL;
 	*out = NULL;
-	if (records == 0 || (records & (records - 1)) || records > (1u << 25))
+	if (records == 0 || (records & (records - 1)) || records > (1u << 24))
 		return KMA_EINVAL;
 	kma_device_guard g(device);
 	if (!g.ok)
@@ -1212,7 +1212,7 @@ extern "C" int kma_c3_queue_run(int kind, uint32_t threads, uint32_t per_thread,
 	kma_chain_log_t log = NULL;
 	if (warp) {
 		uint32_t rec = 1;
-		while (rec < n / 16 && rec < (1u << 25))
+		while (rec < n / 16 && rec < (1u << 24))
 			rec <<= 1;
 		rc = kma_chain_log_create(rec, -1, NULL, &log);
 	}

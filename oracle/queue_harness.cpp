@@ -128,10 +128,16 @@ HostLog g_log;
 const HostLog *log_ptr() { return g_log.mask || !g_log.clq.empty() || !g_log.iq.empty() ? &g_log : nullptr; }
 
 struct Result {
-	uint64_t enq = 0, deq = 0, left = 0, bad = 0, order = 0, timeouts = 0;
+	uint64_t enq = 0, deq = 0, left = 0, bad = 0, order = 0, timeouts = 0, holds = 0;
 };
 
 int g_producers = 0;
+/* MAX_CHAIN or DEQ_BATCH given negative: every chain / every batch has
+ * exactly that many items (a warp's chains, a block's dequeues) */
+bool g_fixed_chain = false, g_fixed_batch = false;
+/* consumers start when every producer is done (config 3's enqueue-then-
+ * dequeue phases: the queue holds whole chains, so batches meet the log) */
+bool g_phased = false;
 
 void split(int threads, int &np, int &nc)
 {
@@ -144,7 +150,7 @@ void split(int threads, int &np, int &nc)
 /* appends[i] / takes[i]: item i's appends and takes */
 struct Book {
 	std::vector<uint64_t> appends, takes;
-	std::atomic<uint64_t> enq{0}, deq{0}, order_bad{0}, tmo{0};
+	std::atomic<uint64_t> enq{0}, deq{0}, order_bad{0}, tmo{0}, holds{0};
 	uint64_t cap; /* more takes than this: the queue hands items out twice */
 	Book(size_t n, uint64_t c) : appends(n, 0), takes(n, 0), cap(c) {}
 	/* a fault is already reported: the threads stop rather than wait out
@@ -192,7 +198,8 @@ void run_clq(int threads, int chains, int maxc, int batch, double recycle, uint6
 			}
 			__atomic_store_n(&v[j]->next, link, __ATOMIC_RELAXED);
 		}
-		if (!kma_q::clq_append<HostOps, LinkAtItem>(&q[0], &q[1], (u64)v[0], (u64)v[len - 1], LIMIT))
+		if (!kma_q::clq_append<HostOps, LinkAtItem>(&q[0], &q[1], (u64)v[0], (u64)v[len - 1], LIMIT,
+							     logged ? kma_q::clq_mark_into(recno) : 0ull))
 			bk.tmo++;
 		bk.enq += len;
 	};
@@ -202,7 +209,7 @@ void run_clq(int threads, int chains, int maxc, int batch, double recycle, uint6
 		std::vector<Item *> v(maxc);
 		uint32_t seq = 0, used = 0;
 		for (int c = 0; c < chains && !bk.runaway(); c++) {
-			int len = 1 + (int)(rnd() % maxc);
+			int len = g_fixed_chain ? maxc : 1 + (int)(rnd() % maxc);
 			for (int j = 0; j < len; j++)
 				v[j] = &mine[used + j];
 			used += len;
@@ -212,6 +219,8 @@ void run_clq(int threads, int chains, int maxc, int batch, double recycle, uint6
 	};
 	auto consumer = [&](int c) {
 		t_rng = seed * 0x9E3779B97F4A7C15ull + 0x2000u + c;
+		while (g_phased && producing.load() != 0)
+			std::this_thread::yield();
 		Orders ord((size_t)np + nc);
 		std::vector<u64> out(batch);
 		std::vector<Item *> back;
@@ -219,7 +228,7 @@ void run_clq(int threads, int chains, int maxc, int batch, double recycle, uint6
 		for (;;) {
 			bool done = producing.load() == 0;
 			bool to = false;
-			uint32_t k = 1 + (uint32_t)(rnd() % batch);
+			uint32_t k = g_fixed_batch ? (uint32_t)batch : 1 + (uint32_t)(rnd() % batch);
 			uint32_t r = kma_q::clq_dequeue_n<HostOps, LinkAtItem>(&q[0], &q[1], out.data(), k, LIMIT, &to,
 									       log_ptr());
 			if (to)
@@ -234,6 +243,7 @@ void run_clq(int threads, int chains, int maxc, int batch, double recycle, uint6
 					back.push_back(it);
 			}
 			bk.deq += r;
+			bk.holds += r ? 1 : 0;
 			if (!back.empty())
 				/* re-appended in chains of at most 32, a warp's */
 				for (size_t o = 0; o < back.size(); o += 32)
@@ -272,6 +282,7 @@ void run_clq(int threads, int chains, int maxc, int batch, double recycle, uint6
 				bad++; /* taken items keep POISON */
 	R.enq = bk.enq;
 	R.deq = bk.deq;
+	R.holds = bk.holds;
 	R.left = left;
 	R.bad = bad;
 	R.order = bk.order_bad;
@@ -321,7 +332,7 @@ void run_iq(int threads, int chains, int maxc, int batch, double recycle, uint64
 		std::vector<uint32_t> v(maxc);
 		uint32_t seq = 0, used = 0;
 		for (int c = 0; c < chains && !bk.runaway(); c++) {
-			int len = 1 + (int)(rnd() % maxc);
+			int len = g_fixed_chain ? maxc : 1 + (int)(rnd() % maxc);
 			for (int j = 0; j < len; j++)
 				v[j] = base + used + j;
 			used += len;
@@ -331,13 +342,15 @@ void run_iq(int threads, int chains, int maxc, int batch, double recycle, uint64
 	};
 	auto consumer = [&](int c) {
 		t_rng = seed * 0x9E3779B97F4A7C15ull + 0x4000u + c;
+		while (g_phased && producing.load() != 0)
+			std::this_thread::yield();
 		Orders ord((size_t)np + nc);
 		std::vector<uint32_t> out(batch), back;
 		uint32_t seq = 0;
 		for (;;) {
 			bool done = producing.load() == 0;
 			bool to = false;
-			uint32_t k = 1 + (uint32_t)(rnd() % batch);
+			uint32_t k = g_fixed_batch ? (uint32_t)batch : 1 + (uint32_t)(rnd() % batch);
 			uint32_t r = kma_q::iq_dequeue_n<HostOps>(q, &ends[0], out.data(), k, LIMIT, &to, log_ptr());
 			if (to)
 				bk.tmo++;
@@ -351,6 +364,7 @@ void run_iq(int threads, int chains, int maxc, int batch, double recycle, uint64
 					back.push_back(idx);
 			}
 			bk.deq += r;
+			bk.holds += r ? 1 : 0;
 			if (!back.empty())
 				/* re-appended in chains of at most 32, a warp's */
 				for (size_t o = 0; o < back.size(); o += 32)
@@ -383,6 +397,7 @@ void run_iq(int threads, int chains, int maxc, int batch, double recycle, uint64
 			bad++;
 	R.enq = bk.enq;
 	R.deq = bk.deq;
+	R.holds = bk.holds;
 	R.left = left;
 	R.bad = bad;
 	R.order = bk.order_bad;
@@ -441,19 +456,29 @@ int main(int argc, char **argv)
 {
 	if (argc == 2 && strcmp(argv[1], "stuck") == 0)
 		return run_stuck();
-	if (argc < 8 || argc > 11) {
+	if (argc < 8 || argc > 12) {
 		fprintf(stderr, "usage: %s clq|iq THREADS CHAINS MAX_CHAIN DEQ_BATCH DELAY_PROB SEED "
-			"[PRODUCERS [RECYCLE [LOG_RECORDS]]]\n       %s stuck\n", argv[0], argv[0]);
+			"[PRODUCERS [RECYCLE [LOG_RECORDS [PHASED]]]]\n       %s stuck\n", argv[0], argv[0]);
 		return 2;
 	}
 	const bool clq = strcmp(argv[1], "clq") == 0;
-	const int threads = atoi(argv[2]), chains = atoi(argv[3]), maxc = atoi(argv[4]), batch = atoi(argv[5]);
+	const int threads = atoi(argv[2]), chains = atoi(argv[3]);
+	int maxc = atoi(argv[4]), batch = atoi(argv[5]);
+	if (maxc < 0) {
+		g_fixed_chain = true;
+		maxc = -maxc;
+	}
+	if (batch < 0) {
+		g_fixed_batch = true;
+		batch = -batch;
+	}
 	g_delay_prob = atof(argv[6]);
 	const uint64_t seed = strtoull(argv[7], NULL, 0);
 	if (argc >= 9)
 		g_producers = atoi(argv[8]);
 	const double recycle = argc >= 10 ? atof(argv[9]) : 0.5;
 	const uint32_t log_records = argc >= 11 ? (uint32_t)strtoul(argv[10], NULL, 0) : 0u;
+	g_phased = argc >= 12 && atoi(argv[11]) != 0;
 	if (log_records) {
 		if (log_records & (log_records - 1))
 			return 2; /* a power of two */
@@ -473,9 +498,10 @@ int main(int argc, char **argv)
 	const bool ok = R.bad == 0 && R.order == 0 && R.timeouts == 0;
 	printf("{\"queue\": \"%s\", \"log_records\": %u, \"log_chains\": %llu, \"threads\": %d, \"appended\": %llu, \"taken\": %llu, \"left\": %llu, "
 	       "\"conservation_faults\": %llu, \"order_faults\": %llu, \"timeouts\": %llu, \"delays\": %llu, "
-	       "\"seconds\": %.3f, \"ok\": %s}\n",
+	       "\"dequeue_calls\": %llu, \"seconds\": %.3f, \"ok\": %s}\n",
 	       clq ? "clq" : "iq", log_records, (unsigned long long)g_log.chains.load(), threads, (unsigned long long)R.enq, (unsigned long long)R.deq,
 	       (unsigned long long)R.left, (unsigned long long)R.bad, (unsigned long long)R.order,
-	       (unsigned long long)R.timeouts, (unsigned long long)g_delays.load(), s, ok ? "true" : "false");
+	       (unsigned long long)R.timeouts, (unsigned long long)g_delays.load(), (unsigned long long)R.holds, s,
+	       ok ? "true" : "false");
 	return ok ? 0 : 1;
 }

@@ -25,7 +25,9 @@ ORACLE = os.path.join(ROOT, "oracle")
 HARNESS = os.path.join(ORACLE, "queue_harness")
 ALGO = os.path.join(ROOT, "include", "kma_queue_algo.cuh")
 
-# threads chains max_chain deq_batch delay_prob seed producers recycle log_records
+# threads chains max_chain deq_batch delay_prob seed producers recycle log_records [phased]
+# (a negative max_chain / deq_batch: every chain / batch exactly that long;
+# phased: consumers start when the producers are done, as config 3 runs)
 CONFIGS = [
     "8 20000 1 1 0.01 1 1 0.5 0",      # single items, one producer: the queue is mostly empty
     "8 20000 4 4 0.01 2 2 0.5 0",
@@ -45,7 +47,46 @@ CONFIGS = [
     "8 5000 32 256 0.02 12 4 0.5 8",
     "8 20000 8 64 0.01 13 2 0.5 1024",
     "8 40000 32 256 0.0005 14 4 0 1024",
+    # warp-sized chains taken by block-sized batches from a full queue:
+    # several whole chains per hold, each reached over its marked link
+    "8 5000 -32 -256 0.02 15 4 0.5 65536 1",
+    "8 5000 -32 -256 0.02 16 4 0.5 16 1",
+    "8 5000 -8 -64 0.01 17 2 0.5 1024 1",
+    "8 5000 32 -256 0.02 19 4 0.5 65536 1",
 ]
+
+# block-sized batches (256) over whole warp chains (32): every chain must
+# come out of its record, eight to a hold of the head, not by walking
+LOG_PATH_CFG = "8 5000 -32 -256 0 15 4 0 65536 1"
+
+
+def log_path_use(binary, kind):
+    """(share of chains taken from their records, chains per dequeue call)"""
+    rc, st = run(binary, kind, LOG_PATH_CFG)
+    assert rc == 0 and st.get("ok"), st
+    return st["log_chains"] / (st["appended"] / 32), st["log_chains"] / st["dequeue_calls"]
+
+
+@pytest.mark.parametrize("kind", ["clq", "iq"])
+def test_block_batches_take_whole_chains_from_the_log(harness, kind):
+    share, per_call = log_path_use(harness, kind)
+    assert share > 0.9 and per_call > 6
+
+def test_log_path_check_sees_a_wrong_record_number(harness, tmp_path):
+    """Plant a wrong record number on the path that reads it from the link
+    into a chain: those records never match, so each hold stops after its
+    first chain, and the chains-per-call figure above collapses (the check
+    above would catch it)."""
+    src = open(ALGO).read()
+    old = "((via_into ? into : l1) >> PTR_BITS) & 0x3FFFu"
+    assert src.count(old) == 1
+    d = tmp_path / "into"
+    d.mkdir()
+    (d / "kma_queue_algo.cuh").write_text(src.replace(old, "((via_into ? into + (1ull << PTR_BITS) : l1) >> PTR_BITS) & 0x3FFFu"))
+    binary = str(d / "h")
+    subprocess.run([os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-pthread", f"-I{d}", "-o", binary,
+                    os.path.join(ORACLE, "queue_harness.cpp")], check=True)
+    assert log_path_use(binary, "clq")[1] < 2
 
 
 def have_compiler() -> bool:
@@ -92,8 +133,8 @@ MUTANTS = {
     # link after the previous tail with a plain store: a dequeuer's hold
     # of that link (POISON) is overwritten, and its restore then cuts the chain
     "append_link_store": ("clq", "8 20000 1 1 0.01 1 1 0.5",
-                          "const u64 old = O::cas(pl, 0ull, first);",
-                          "const u64 old = 0; O::st(pl, first);"),
+                          "const u64 old = O::cas(pl, 0ull, first | into);",
+                          "const u64 old = 0; O::st(pl, first | into);"),
     # no check that the held item is still the head (ABA after recycling)
     "no_head_recheck": ("clq", "8 20000 4 4 0.01 2 2 0.5",
                         "\t\tif (O::ld(headw) != h) {\n\t\t\tO::st(hl, nx);",
