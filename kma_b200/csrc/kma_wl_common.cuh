@@ -107,12 +107,13 @@ __device__ __forceinline__ uint32_t verify_share(uint32_t r, uint32_t width, con
 	return bad;
 }
 
-/* Vectors each lane has in flight per batch of coop_verify_rows (4:
- * config 2's rounds kernel, 64 registers, measured 8.73 against 8.90 ms
- * per launch for the block-by-block loop; 6 and 8 spill more and measured
- * 9.57 and 10.02 ms). */
+/* Vectors each lane has in flight per batch of coop_verify_rows.  With the
+ * streaming payload hints, config 2's rounds kernel (64 registers)
+ * measured 7.78 / 7.93 / 8.14 / 8.13 ms per launch at 3 / 2 / 1 / 4, and
+ * 8.32 ms block by block (0): deeper batches cost more spills than they
+ * hide latency. */
 #ifndef WL_VERIFY_SLOTS
-#define WL_VERIFY_SLOTS 4
+#define WL_VERIFY_SLOTS 3
 #endif
 
 /* Verify every lane's block (p may be NULL) against its tag; true in the
