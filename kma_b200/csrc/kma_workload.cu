@@ -323,7 +323,7 @@ __device__ __forceinline__ void flush_counters(const wl_dev &w, uint32_t mask, u
  * (Launching one thread per item instead lets early waves finish all
  * their rounds and pin their last live blocks while later waves start,
  * which fragments the heap far beyond what concurrent items do.) */
-template <int MODE>
+template <int MODE, bool C2>
 __global__ void __launch_bounds__(256, 4) k_wl_rounds(kma_heap *h, wl_dev w, uint32_t nrounds, int drain)
 {
 	const uint32_t mask = 0xffffffffu;
@@ -335,7 +335,10 @@ __global__ void __launch_bounds__(256, 4) k_wl_rounds(kma_heap *h, wl_dev w, uin
 		s_hint[threadIdx.x >> 5][lane] = 0;
 	__syncwarp();
 	wl_counters ct = {0, 0, 0, 0, 0, 0, {0, 0, 0, 0}, {{0, 0, 0, 0, 0, 0, 0, 0}}, s_hint[threadIdx.x >> 5]};
-	const bool c2 = w.program == KMA_WL_C2;
+	/* one kernel per program: a kernel carrying both programs' paths
+	 * spilled 148 bytes per thread at the 64-register cap, the config-2
+	 * one alone 48 */
+	const bool c2 = C2;
 	{
 		for (uint32_t r = 0; r <= nrounds; r++) {
 			if (r == nrounds && !(drain && c2))
@@ -362,6 +365,22 @@ __global__ void __launch_bounds__(256, 4) k_wl_rounds(kma_heap *h, wl_dev w, uin
 		}
 	}
 	flush_counters(w, mask, lane, ct);
+}
+
+/* The rounds kernel of a call style for a program (config 2, or config 1). */
+template <int MODE>
+const void *wl_rounds_fn(bool c2)
+{
+	return c2 ? (const void *)k_wl_rounds<MODE, true> : (const void *)k_wl_rounds<MODE, false>;
+}
+template <int MODE>
+void wl_rounds_launch(bool c2, uint32_t nb, uint32_t bd, cudaStream_t st, kma_heap *h, const wl_dev &d,
+		      uint32_t nrounds, int drain)
+{
+	if (c2)
+		k_wl_rounds<MODE, true><<<nb, bd, 0, st>>>(h, d, nrounds, drain);
+	else
+		k_wl_rounds<MODE, false><<<nb, bd, 0, st>>>(h, d, nrounds, drain);
 }
 
 /* One thread runs every item (round_major: round by round). */
@@ -562,18 +581,18 @@ static int wl_launch(kma_wl_t w, uint32_t nrounds, int mode, uint32_t bd, int dr
 	uint32_t nb = wl_blocks(w->d.items, bd);
 	/* persistent grid: no more blocks than stay resident on all SMs */
 	int per_sm = 0, sms = 0;
-	const void *fns[4] = {(const void *)k_wl_rounds<0>, (const void *)k_wl_rounds<1>,
-			      (const void *)k_wl_rounds<2>, (const void *)k_wl_rounds<3>};
+	const bool c2 = w->d.program == KMA_WL_C2;
+	const void *fns[4] = {wl_rounds_fn<0>(c2), wl_rounds_fn<1>(c2), wl_rounds_fn<2>(c2), wl_rounds_fn<3>(c2)};
 	KMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fns[mode], (int)bd, 0));
 	KMA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, w->heap->device));
 	uint64_t resident = (uint64_t)(per_sm > 0 ? per_sm : 1) * (uint64_t)(sms > 0 ? sms : 1);
 	if (nb > resident)
 		nb = (uint32_t)resident;
 	switch (mode) {
-	case 0: k_wl_rounds<0><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain); break;
-	case 1: k_wl_rounds<1><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain); break;
-	case 2: k_wl_rounds<2><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain); break;
-	default: k_wl_rounds<3><<<nb, bd, 0, st>>>(w->heap->dh, w->d, nrounds, drain); break;
+	case 0: wl_rounds_launch<0>(c2, nb, bd, st, w->heap->dh, w->d, nrounds, drain); break;
+	case 1: wl_rounds_launch<1>(c2, nb, bd, st, w->heap->dh, w->d, nrounds, drain); break;
+	case 2: wl_rounds_launch<2>(c2, nb, bd, st, w->heap->dh, w->d, nrounds, drain); break;
+	default: wl_rounds_launch<3>(c2, nb, bd, st, w->heap->dh, w->d, nrounds, drain); break;
 	}
 	KMA_CUDA(cudaGetLastError());
 	return KMA_OK;
@@ -847,17 +866,17 @@ extern "C" int kma_wl_run_noalloc(kma_heap_t h, int program, uint64_t items, con
 	} else {
 		uint32_t nb = wl_blocks(items, 256);
 		int per_sm = 0, sms = 0;
-		const void *fn = mode == KMA_MODE_WARP ? (const void *)k_wl_rounds<KMA_MODE_WARP>
-						       : (const void *)k_wl_rounds<KMA_MODE_PLAIN>;
+		const bool c2 = d.program == KMA_WL_C2;
+		const void *fn = mode == KMA_MODE_WARP ? wl_rounds_fn<KMA_MODE_WARP>(c2) : wl_rounds_fn<KMA_MODE_PLAIN>(c2);
 		KMA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
 		KMA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
 		uint64_t resident = (uint64_t)(per_sm > 0 ? per_sm : 1) * (uint64_t)(sms > 0 ? sms : 1);
 		if (nb > resident)
 			nb = (uint32_t)resident;
 		if (mode == KMA_MODE_WARP)
-			k_wl_rounds<KMA_MODE_WARP><<<nb, 256, 0, st>>>(h->dh, d, nrounds, 1);
+			wl_rounds_launch<KMA_MODE_WARP>(c2, nb, 256, st, h->dh, d, nrounds, 1);
 		else
-			k_wl_rounds<KMA_MODE_PLAIN><<<nb, 256, 0, st>>>(h->dh, d, nrounds, 1);
+			wl_rounds_launch<KMA_MODE_PLAIN>(c2, nb, 256, st, h->dh, d, nrounds, 1);
 	}
 	k_noalloc_finish<<<1, 1024, 0, st>>>(d.stats, hashes_dev, items, stats_dev);
 	KMA_CUDA(cudaGetLastError());
