@@ -32,10 +32,11 @@
  * record's number and k.  A dequeue that finds a marked link at the head
  * reads the record and checks every link it names with loads that do not
  * depend on one another (one round trip, not k), and takes the whole
- * chain with one move of the head.  A record is only a hint: records are
- * reused round robin, so a dequeue takes a chain from its record only
- * when the queue's current links say exactly what the record says, and
- * walks otherwise.
+ * chain with one move of the head; a dequeue that wants more (the block
+ * forms) goes on to the next logged chains under the same hold.  A record
+ * is only a hint: records are reused round robin, so a dequeue takes a
+ * chain from its record only when the queue's current links say exactly
+ * what the record says, and walks otherwise.
  *
  * Log policy `LG` (a null pointer, or the type no_log: no log; `enabled`
  * false compiles the log code out) provides the slot of record `recno`

@@ -25,16 +25,27 @@
  *     log is overwritten while its chains are still queued, so dequeues
  *     meet stale records), and dequeues take chains from their records.
  *
- *   queue_harness clq|iq THREADS CHAINS MAX_CHAIN DEQ_BATCH DELAY_PROB SEED [PRODUCERS [RECYCLE [LOG_RECORDS]]]
+ *   - stuck queues (`queue_harness stuck`): a dequeuer that died holding
+ *     the head, an append that exchanged the tail and never linked, an
+ *     indexed head left held: every dequeue must give up within its limit
+ *     and report it.
+ *
+ *   queue_harness clq|iq THREADS CHAINS MAX_CHAIN DEQ_BATCH DELAY_PROB SEED
+ *                 [PRODUCERS [RECYCLE [LOG_RECORDS [PHASED]]]]
+ *   queue_harness stuck
  *
  * PRODUCERS of the threads (default half) append CHAINS fresh chains of
  * 1..MAX_CHAIN items each; the rest take batches of 1..DEQ_BATCH until
- * the producers are done and the queue is empty.  With few producers the
- * queue is mostly empty, so the empty <-> one-item transitions and the
- * append window are met all the time.  Prints one JSON line; exits 0 when
- * every check passed.  The reference's own queues are the parity oracle
- * (serial replays against tests/golden); this program checks this build's
- * concurrent behaviour.
+ * the producers are done and the queue is empty (a negative MAX_CHAIN or
+ * DEQ_BATCH: exactly that many, as warps append and blocks dequeue).
+ * With few producers the queue is mostly empty, so the empty <-> one-item
+ * transitions and the append window are met all the time; PHASED 1 holds
+ * the consumers back until the producers are done (config 3's order), so
+ * batches meet whole logged chains and take several per hold.  Prints one
+ * JSON line (with the chains taken from records and the dequeue calls
+ * that took items); exits 0 when every check passed.  The reference's own
+ * queues are the parity oracle (serial replays against tests/golden);
+ * this program checks this build's concurrent behaviour.
  */
 #include <algorithm>
 #include <atomic>
