@@ -228,11 +228,36 @@ __device__ __forceinline__ uint32_t cas_relaxed(uint32_t *p, uint32_t cmp, uint3
 		     : "=r"(old) : "l"(p), "r"(cmp), "r"(val) : "memory");
 	return old;
 }
-__device__ __forceinline__ uint32_t or_relaxed(uint32_t *p, uint32_t v)
+/* Allocation-bitmap words sit at the superblock tails, in lines they
+ * share with payload that the workloads write and read as evict-first
+ * (streaming); their atomics ask L2 to keep the line (evict_last): the
+ * claims and frees then find it in L2 (config 2's rounds launch measured
+ * 7.58 vs 7.66 ms).  A cache hint only: ordering and results unchanged. */
+__device__ __forceinline__ unsigned long long keep_policy()
+{
+	unsigned long long pol;
+	asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+	return pol;
+}
+__device__ __forceinline__ uint32_t bm_or(uint32_t *p, uint32_t v)
 {
 	uint32_t old;
-	asm volatile("atom.relaxed.gpu.global.or.b32 %0, [%1], %2;"
-		     : "=r"(old) : "l"(p), "r"(v) : "memory");
+	asm volatile("atom.relaxed.gpu.global.or.L2::cache_hint.b32 %0, [%1], %2, %3;"
+		     : "=r"(old) : "l"(p), "r"(v), "l"(keep_policy()) : "memory");
+	return old;
+}
+__device__ __forceinline__ uint32_t bm_and(uint32_t *p, uint32_t v)
+{
+	uint32_t old;
+	asm volatile("atom.relaxed.gpu.global.and.L2::cache_hint.b32 %0, [%1], %2, %3;"
+		     : "=r"(old) : "l"(p), "r"(v), "l"(keep_policy()) : "memory");
+	return old;
+}
+__device__ __forceinline__ uint32_t bm_and_release(uint32_t *p, uint32_t v)
+{
+	uint32_t old;
+	asm volatile("atom.release.gpu.global.and.L2::cache_hint.b32 %0, [%1], %2, %3;"
+		     : "=r"(old) : "l"(p), "r"(v), "l"(keep_policy()) : "memory");
 	return old;
 }
 __device__ __forceinline__ uint32_t cas_release(uint32_t *p, uint32_t cmp, uint32_t val)
@@ -258,13 +283,6 @@ __device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long l
 __device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v)
 {
 	asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-__device__ __forceinline__ uint32_t and_release(uint32_t *p, uint32_t v)
-{
-	uint32_t old;
-	asm volatile("atom.release.gpu.global.and.b32 %0, [%1], %2;"
-		     : "=r"(old) : "l"(p), "r"(v) : "memory");
-	return old;
 }
 __device__ __forceinline__ uint32_t lane_id()
 {
@@ -585,7 +603,7 @@ __device__ __forceinline__ void *sb_get_block(kma_heap *h, uint32_t s, uint32_t 
 		while (cand) {
 			uint32_t b = __ffs(cand) - 1;
 			uint32_t bit = 1u << b;
-			uint32_t old = or_relaxed(wp, bit);
+			uint32_t old = bm_or(wp, bit);
 			if (!(old & bit)) {
 				unsigned char *p = sb + KMA_SB_HDR + (size_t)(k * 32 + b) * size;
 				*reinterpret_cast<uint32_t *>(p) = hint;
@@ -733,7 +751,7 @@ __device__ inline void kma_free(kma_heap *h, void *p)
 		return;
 	}
 	*reinterpret_cast<volatile uint32_t *>(p) = cur;
-	uint32_t old = and_release(wp, ~bit);
+	uint32_t old = bm_and_release(wp, ~bit);
 	if (!(old & bit)) {
 		set_err(h, KMA_ERR_BADFREE); /* a concurrent double free */
 		return;
@@ -969,7 +987,7 @@ __device__ __forceinline__ uint32_t warp_claim_step(kma_heap *h, warp_resv &r, u
 	}
 	uint32_t got = 0;
 	if (pick) {
-		uint32_t old = or_relaxed(wp, pick);
+		uint32_t old = bm_or(wp, pick);
 		got = pick & ~old;
 		r.kword = k;
 		r.known = old | pick;
@@ -1111,7 +1129,7 @@ __device__ inline void kma_free_warp(kma_heap *h, void *p)
 			uint32_t cur = ld_relaxed(wp);
 			if (cur & bit) {
 				*reinterpret_cast<volatile uint32_t *>(p) = cur;
-				old = and_release(wp, ~mask);
+				old = bm_and_release(wp, ~mask);
 			} else {
 				old = cur;
 			}
@@ -1119,7 +1137,7 @@ __device__ inline void kma_free_warp(kma_heap *h, void *p)
 	} else if (valid && lane == wleader) {
 		/* several blocks at once: freed memory has no defined contents,
 		 * so the residue (a load, a store and a fence) is skipped */
-		old = atomicAnd(wp, ~mask);
+		old = bm_and(wp, ~mask);
 	}
 	old = __shfl_sync(active, old, wleader);
 	bool good = valid && (old & bit);
