@@ -51,3 +51,12 @@ def test_host_only_calls_without_gpu():
     cfg = _lib.KmaConfig(16, 11, 0, -1)  # superblocks below 4 KiB are rejected
     assert L.kma_create_ex(ctypes.byref(cfg), None, ctypes.byref(h)) == _lib.KMA_EINVAL
     assert L.kma_destroy(None) == _lib.KMA_EINVAL
+    # queue entry points that refuse their arguments before any CUDA call
+    log = ctypes.c_void_p()
+    assert L.kma_chain_log_create(1 << 25, -1, None, ctypes.byref(log)) == _lib.KMA_EINVAL  # above 2^24 records
+    assert L.kma_chain_log_create(3, -1, None, ctypes.byref(log)) == _lib.KMA_EINVAL        # not a power of two
+    taken, flags = ctypes.c_int64(), ctypes.c_uint32()
+    assert L.kma_debug_queue_stuck_dequeue(1, 1, 64, -1, ctypes.byref(taken),
+                                           ctypes.byref(flags)) == _lib.KMA_EINVAL  # no such indexed-queue case
+    assert L.kma_debug_queue_stuck_dequeue(0, 0, 0, -1, ctypes.byref(taken),
+                                           ctypes.byref(flags)) == _lib.KMA_EINVAL  # spin limit 0
