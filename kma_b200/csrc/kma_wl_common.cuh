@@ -79,8 +79,11 @@ __device__ __forceinline__ void coop_fill(uint32_t mask, uint32_t lane, void *p,
 		pl_st(&w[i], tag);
 }
 
-/* Blocks of at least this many bytes are verified by the whole warp. */
+/* Blocks of at least this many bytes are verified by the whole warp
+ * (config 2's rounds kernel: 128 and 256 measured alike, 512 2% slower). */
+#ifndef WL_COOP_BYTES
 #define WL_COOP_BYTES 256u
+#endif
 
 /* The share of the r-th of `width` calling lanes in verifying block p (nw
  * words) cooperatively: head words up to the 16-byte boundary, 16-byte
