@@ -17,9 +17,13 @@ and has no exchange step).  It also reports the plain per-thread kernel on
 the same GPU, the roofline of the dominant kernel, the CPU baseline, the
 end-to-end figure through the host-buffer C ABI call, the invariant check
 of one extra step, and (under "forms") the other configurations: the
-lock-free structures (config 3), the autotuned batched form (config 4) and
-the served form's p50/p99 latency at swept arrival rates (config 5).  The reference arm times the reference's own
-kma.cl built as host C (oracle/_ref) on the host cores.
+lock-free structures (config 3: one clQueue and one indexed queue at full
+size through the warp and block forms, and the tree), the autotuned
+batched form (config 4) and the served form's p50/p99 latency at swept
+arrival rates (config 5), each beside the plain per-thread calls on the
+same work, with PMA arms where the PMA heap applies, and the graph build
+of the reference's tree driver.  The reference arm times the reference's
+own kma.cl built as host C (oracle/_ref) on the host cores.
 """
 from __future__ import annotations
 
