@@ -122,6 +122,16 @@ int kma_iqueue_replay_host(uint32_t n_items, uint32_t stride_l2, const int64_t *
 int kma_debug_queue_stuck_dequeue(int kind, int state, uint32_t spin_limit, int device, int64_t *taken,
 				  uint32_t *flags);
 
+/* No counterpart in the reference.  FIFO order through the warp and block
+ * forms, in one block of `tpb` threads (a multiple of 32, at most 512):
+ * for each of `calls` rounds the block's warps append 32 items each, one
+ * warp after another (warp forms, chain log on); then the block makes
+ * `calls` block-form dequeues.  out[c * tpb + t] = the item thread t got
+ * in dequeue c, as its enqueue number (0, 1, ...; the indexed queue's
+ * initial dummy comes out first as -2), -1 for NULL.  *err: error flags.
+ * kind: KMA_C3_CLQUEUE or KMA_C3_IQUEUE. */
+int kma_debug_queue_block_fifo(int kind, uint32_t tpb, uint32_t calls, int device, int64_t *out, uint32_t *err);
+
 /* ---- clTree ---------------------------------------------------------- */
 /* One-thread replay of a clTree (clTree.cl:27-74) with one 24-byte node per
  * op that the call allocates: ops (0, key) add -> 1 inserted, 0 exists,

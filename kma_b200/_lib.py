@@ -157,6 +157,7 @@ SIGNATURES = [
     ("kma_wl_live", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("kma_debug_set_class_word", c_int, [c_void_p, c_uint32, c_uint32, c_void_p]),
     ("kma_debug_queue_stuck_dequeue", c_int, [c_int, c_int, c_uint32, c_int, c_void_p, c_void_p]),
+    ("kma_debug_queue_block_fifo", c_int, [c_int, c_uint32, c_uint32, c_int, c_void_p, c_void_p]),
     ("kma_bench_atomics", c_int, [c_int, c_uint64, c_uint32, c_uint32, c_void_p, POINTER(c_float)]),
     # include/kma_structs.h
     ("kma_pma_create", c_int, [c_uint64, c_int, c_void_p, POINTER(c_void_p)]),

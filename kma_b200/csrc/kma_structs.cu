@@ -456,6 +456,110 @@ __global__ void k_dbg_stuck_iq(uint32_t limit, kma_iqueue *q, int64_t *out)
 }
 } /* namespace */
 
+namespace {
+/* one block: warps append 32 items each, in warp order, `calls` times;
+ * then `calls` block-form dequeues */
+__global__ void __launch_bounds__(512) k_dbg_fifo_clq(kma_clqueue *q, unsigned char *items, uint32_t calls, int64_t *out, uint32_t *err,
+			       const kma_chain_log *log)
+{
+	__shared__ unsigned long long smem[512 + 1];
+	const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+	for (uint32_t c = 0; c < calls; c++)
+		for (uint32_t w = 0; w < nw; w++) {
+			if (wid == w) {
+				const size_t i = (size_t)c * blockDim.x + w * 32 + lane;
+				kma_clqueue_enqueue_warp(q, (kma_clqueue_item *)(items + i * QITEM), err, KMA_STRUCT_SPIN,
+							 const_cast<kma_chain_log *>(log));
+			}
+			__syncthreads();
+		}
+	for (uint32_t c = 0; c < calls; c++) {
+		kma_clqueue_item *it = kma_clqueue_dequeue_block(q, true, smem, err, KMA_STRUCT_SPIN, log);
+		out[(size_t)c * blockDim.x + tid] = it ? (int64_t)(((unsigned char *)it - items) / QITEM) : -1;
+	}
+}
+__global__ void __launch_bounds__(512) k_dbg_fifo_iq(kma_iqueue *q, uint32_t calls, int64_t *out)
+{
+	__shared__ unsigned long long smem[512 + 1];
+	const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+	for (uint32_t c = 0; c < calls; c++)
+		for (uint32_t w = 0; w < nw; w++) {
+			if (wid == w) {
+				/* item i of the enqueue order is array item i + 2 (item 1 is the dummy) */
+				const size_t i = (size_t)c * blockDim.x + w * 32 + lane;
+				kma_iqueue_enqueue_warp_shard(q, q->base + ((i + 1) << q->stride_l2), 0);
+			}
+			__syncthreads();
+		}
+	for (uint32_t c = 0; c < calls; c++) {
+		unsigned char *it = (unsigned char *)kma_iqueue_dequeue_block(q, true, smem);
+		out[(size_t)c * blockDim.x + tid] =
+			!it ? -1 : (it == q->base ? -2 : (int64_t)((it - q->base) >> q->stride_l2) - 1);
+	}
+}
+} /* namespace */
+
+extern "C" int kma_debug_queue_block_fifo(int kind, uint32_t tpb, uint32_t calls, int device, int64_t *out,
+		uint32_t *err)
+{
+	if (!out || !err || tpb == 0 || tpb % 32 || tpb > 512 || calls == 0 || calls > 1024 ||
+	    (kind != KMA_C3_CLQUEUE && kind != KMA_C3_IQUEUE))
+		return KMA_EINVAL;
+	kma_device_guard g(device);
+	if (!g.ok)
+		return KMA_ENODEV;
+	const size_t n = (size_t)tpb * calls;
+	dev_bufs b;
+	int64_t *dout = b.alloc<int64_t>(n * 8);
+	uint32_t *derr = b.alloc<uint32_t>(4);
+	unsigned char *items = b.alloc<unsigned char>((n + 2) * QITEM);
+	if (!dout || !derr || !items)
+		return KMA_ENOMEM;
+	KMA_CUDA(cudaMemset(derr, 0, 4));
+	KMA_CUDA(cudaMemset(items, 0, (n + 2) * QITEM));
+	kma_chain_log_t log = NULL;
+	uint32_t rec = 1;
+	while (rec < n / 32 + 1)
+		rec <<= 1;
+	int rc = kma_chain_log_create(rec, -1, NULL, &log);
+	if (rc != KMA_OK)
+		return rc;
+	uint32_t e = 0;
+	if (kind == KMA_C3_CLQUEUE) {
+		kma_clqueue *q = b.alloc<kma_clqueue>(sizeof(kma_clqueue));
+		if (!q) {
+			kma_chain_log_destroy(log);
+			return KMA_ENOMEM;
+		}
+		cudaMemset(q, 0, sizeof(kma_clqueue));
+		k_dbg_fifo_clq<<<1, tpb>>>(q, items, calls, dout, derr, kma_chain_log_device_ptr(log));
+		if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+			rc = KMA_ECUDA;
+		if (rc == KMA_OK && cudaMemcpy(&e, derr, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+			rc = KMA_ECUDA;
+	} else {
+		kma_iqueue_t q = NULL;
+		rc = kma_iqueue_create(items, 4, (uint32_t)n + 1, items, 1, -1, NULL, &q);
+		if (rc == KMA_OK)
+			rc = kma_iqueue_set_chain_log(q, log, NULL);
+		if (rc == KMA_OK) {
+			k_dbg_fifo_iq<<<1, tpb>>>(q->dq, calls, dout);
+			if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+				rc = KMA_ECUDA;
+		}
+		if (rc == KMA_OK)
+			rc = kma_iqueue_error_flags(q, NULL, &e, 0);
+		if (q)
+			kma_iqueue_destroy(q);
+	}
+	kma_chain_log_destroy(log);
+	if (rc != KMA_OK)
+		return rc;
+	KMA_CUDA(cudaMemcpy(out, dout, n * 8, cudaMemcpyDeviceToHost));
+	*err = e;
+	return KMA_OK;
+}
+
 extern "C" int kma_debug_queue_stuck_dequeue(int kind, int state, uint32_t spin_limit, int device, int64_t *taken,
 		uint32_t *flags)
 {

@@ -289,6 +289,30 @@ def test_gpu_stuck_queue_dequeue_gives_up_and_flags(kind, state):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kind", [0, 1], ids=["clqueue", "iqueue"])
+@pytest.mark.parametrize("tpb,calls", [(256, 4), (512, 3), (64, 8)])
+def test_gpu_block_form_keeps_fifo_order(kind, tpb, calls):
+    """Warps append their chains one after another (warp forms, chain log),
+    then the block takes them back with the block form: each call returns
+    exactly the next tpb items in queue order, and the lanes of a warp get
+    consecutive items (the indexed queue hands out its initial dummy first,
+    as the reference's does)."""
+    import ctypes
+    from kma_b200._lib import lib
+    out = np.zeros(tpb * calls, np.int64)
+    err = ctypes.c_uint32(0)
+    assert lib().kma_debug_queue_block_fifo(kind, tpb, calls, -1, out.ctypes.data, ctypes.byref(err)) == 0
+    assert err.value == 0
+    pos = out.copy() if kind == 0 else np.where(out == -2, 0, out + 1)  # queue positions
+    assert (out != -1).all()
+    pos = pos.reshape(calls, tpb)
+    for c in range(calls):
+        np.testing.assert_array_equal(np.sort(pos[c]), np.arange(c * tpb, (c + 1) * tpb))
+        warps = pos[c].reshape(-1, 32)
+        np.testing.assert_array_equal(warps - warps[:, :1], np.tile(np.arange(32), (tpb // 32, 1)))
+
+
+@pytest.mark.gpu
 def test_gpu_c3_tree_equals_sequential_replay():
     from kma_b200 import structs
     rng = np.random.default_rng(0xC3)
