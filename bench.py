@@ -306,7 +306,10 @@ def measure_forms(quick: bool = False) -> dict:
                 "exhausted": e["nulls"] - e["refused"]}
     c4 = {"jobs": 64, "work_items": int(t.sum()), "rounds": 16, "heap_bytes": 16 << 30,
           "best": {"sb_size": b["sb_size"], "block_dim": b["block_dim"], "cache_depth": b["cache_depth"],
-                   "mops": b["mops"], "ms_per_launch": b["ms"], **nulls(b), "bad_tags": b["bad_tags"]},
+                   "mops": b["mops"], "ms_per_launch": b["ms"], **nulls(b), "bad_tags": b["bad_tags"],
+                   # algorithmic payload bytes (tag fill + verify, counted by the kernel) per launch
+                   "payload_gbs": round((b["fill_bytes"] + b["verify_bytes"]) / b["ms"] / 1e6, 1),
+                   "hbm_frac": round((b["fill_bytes"] + b["verify_bytes"]) / b["ms"] / 1e6 / peaks()["hbm_gbs"], 4)},
           "grid": [[e["sb_size"], e["block_dim"], e["cache_depth"], e["mops"], e["serves_all"],
                     round(e["nulls"] / e["mallocs"], 4), e["refused"]] for e in entries],
           "grid_cols": ["sb_size", "block_dim", "cache_depth", "mops", "serves_all", "null_frac", "refused"],
