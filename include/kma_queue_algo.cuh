@@ -62,8 +62,10 @@
 
 #if defined(__CUDACC__)
 #define KQ_FN __device__ __forceinline__
+#define KQ_UNROLL _Pragma("unroll")
 #else
 #define KQ_FN inline
+#define KQ_UNROLL
 #endif
 
 namespace kma_q {
@@ -152,7 +154,7 @@ KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32
 	uint32_t m = len < k ? len : k;
 	const u64 *rec = log->clq_record(recno);
 	u64 item[LOG_CHAIN_MAX];
-#pragma unroll
+KQ_UNROLL
 	for (uint32_t j = 0; j < LOG_CHAIN_MAX; j++)
 		item[j] = j <= m && j < len ? LG::ld(rec + j) : 0ull;
 	if (via_into)
@@ -164,7 +166,7 @@ KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32
 	 * filled, or is refilling): none may be followed before it is known
 	 * to be an item */
 	bool ok = true;
-#pragma unroll
+KQ_UNROLL
 	for (uint32_t j = 2; j < LOG_CHAIN_MAX; j++)
 		ok &= !(j < m && item[j] <= POISON);
 	if (!ok)
@@ -172,11 +174,11 @@ KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32
 	/* each item's link must name the next item (for the last one taken:
 	 * the new head) */
 	u64 nxs[LOG_CHAIN_MAX];
-#pragma unroll
+KQ_UNROLL
 	for (uint32_t j = 2; j < LOG_CHAIN_MAX; j++)
 		nxs[j] = j < m ? O::ld_rlx(L::at(item[j])) : 0ull;
 	u64 last = m == 1 ? second : (m == 2 ? l1 : 0ull);
-#pragma unroll
+KQ_UNROLL
 	for (uint32_t j = 2; j < LOG_CHAIN_MAX; j++) {
 		if (j + 1 < m)
 			ok &= nxs[j] != POISON && qp_ptr(nxs[j]) == item[j + 1];
@@ -196,7 +198,7 @@ KQ_FN uint32_t clq_chain_from_log(const LG *log, u64 hp, u64 v, u64 *out, uint32
 	} else if (nh_link) {
 		*nh_link = last;
 	}
-#pragma unroll
+KQ_UNROLL
 	for (uint32_t j = 0; j < LOG_CHAIN_MAX; j++)
 		if (j < m)
 			out[j] = item[j];
@@ -431,19 +433,19 @@ KQ_FN uint32_t iq_chain_from_log(const Q &q, const LG *log, uint32_t h0, u64 l0,
 	uint32_t m = len < k ? len : k;
 	const uint32_t *rec = log->iq_record(recno);
 	uint32_t item[LOG_CHAIN_MAX];
-#pragma unroll
+KQ_UNROLL
 	for (uint32_t j = 0; j < LOG_CHAIN_MAX; j++)
 		item[j] = j <= m && j < len ? LG::ld(rec + j) : 0u;
 	const uint32_t after = m < len ? item[m < LOG_CHAIN_MAX ? m : 0] : 0u;
 	if (item[0] != h0 || (m > 1 && item[1] != tw_idx(l0)) || (m == 1 && len > 1 && after != tw_idx(l0)))
 		return 0;
 	uint32_t nxs[LOG_CHAIN_MAX];
-#pragma unroll
+KQ_UNROLL
 	for (uint32_t j = 1; j < LOG_CHAIN_MAX; j++)
 		nxs[j] = j < m ? tw_idx(O::ld_rlx(q.link(item[j]))) : 0u;
 	bool ok = true;
 	uint32_t next = m == 1 ? tw_idx(l0) : 0u;
-#pragma unroll
+KQ_UNROLL
 	for (uint32_t j = 1; j < LOG_CHAIN_MAX; j++) {
 		if (j + 1 < m)
 			ok &= nxs[j] == item[j + 1];
@@ -465,7 +467,7 @@ KQ_FN uint32_t iq_chain_from_log(const Q &q, const LG *log, uint32_t h0, u64 l0,
 	const uint32_t off = lead ? 1u : 0u;
 	if (lead)
 		out[0] = lead;
-#pragma unroll
+KQ_UNROLL
 	for (uint32_t j = 0; j < LOG_CHAIN_MAX; j++)
 		if (j < m)
 			out[j + off] = item[j];
